@@ -1,0 +1,113 @@
+/*
+ * rhmc_b200.h -- C ABI of librhmc_b200, the B200 (sm_100a) implementation of the RHMC hot
+ * path of coppolachan/RHMC-on-GPU: even/odd staggered Dslash, multi-shift CG on
+ * M^dag M + sigma_i, fermion force, gauge-force staples and the SU(3) momentum/link update.
+ *
+ * Plain C types only.  Every function returns an int status (RHMC_OK or a negative
+ * RHMC_ERR_*); rhmc_last_error() describes the last failure of the calling thread.
+ * Device work is issued on the context's stream (rhmc_set_stream); functions that return
+ * host values synchronise that stream first.
+ *
+ * Field layouts at this boundary are the reference's CPU layouts (complex = two doubles):
+ *   links, momenta, ipdot : complex[4V][3][3], index mu*V + site   (Conf::u_work,
+ *                           include/configuration.h:9-10; Momenta, Ipdot)
+ *   spinor (one parity)   : complex[Vh][3]                        (Fermion, lib/Action/fermions.h:12)
+ * with sites numbered even-first (lib/Main/Geometry/geometry.cc:5-11,86) and the staggered
+ * phases folded into the links (lib/Main/Conf/conf.cc:36,49).
+ * "Internal" spinors are the device layout the kernels use: colour planes [3][Vh] of
+ * complex (double2 for FP64 formats, float2 for FP32 formats); n right-hand sides are
+ * consecutive spinors.
+ *
+ * The reference's own extern "C" GPU entry points (the lib/Cuda headers) are provided, with their
+ * signatures and semantics, by rhmc_legacy.h.
+ */
+#ifndef RHMC_B200_H
+#define RHMC_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct rhmc_ctx rhmc_ctx;
+
+enum {
+    RHMC_OK = 0,
+    RHMC_ERR_ARG = -1,       /* invalid argument (null pointer, bad size, bad enum) */
+    RHMC_ERR_CUDA = -2,      /* a CUDA runtime call failed */
+    RHMC_ERR_MAXITER = -3,   /* a solver hit its iteration cap (reference: exit(1), cu_inverter.cc:62-69) */
+    RHMC_ERR_NONFINITE = -4, /* NaN/Inf detected in a solver reduction */
+    RHMC_ERR_STATE = -5      /* call out of order (e.g. no gauge field set) */
+};
+
+/* Link storage formats used by the Dslash kernels (derived from the FP64 master copy). */
+enum {
+    RHMC_LINKS_F64_18 = 0, /* FP64, all 18 reals */
+    RHMC_LINKS_F64_12 = 1, /* FP64, rows 0-1; row 2 = eta*conj(row0 x row1) (lib/Cuda/cuda_rhmc.cuh:32-45) */
+    RHMC_LINKS_F32_18 = 2, /* FP32, all 18 reals */
+    RHMC_LINKS_F32_12 = 3  /* FP32, rows 0-1, reconstructed */
+};
+
+enum { RHMC_HOST = 0, RHMC_DEVICE = 1 };
+
+/* Run parameters; the reference fixes them at compile time (include/parameters.h:7-76). */
+typedef struct {
+    int nx, ny, nz, nt; /* lattice extents, all even (parameters.h:7-10) */
+    int ferm_temp_bc;   /* 0: antiperiodic fermion time b.c. (parameters.h:29) */
+    double mass;        /* bare staggered mass (parameters.h:16) */
+    double beta;        /* Wilson gauge coupling (parameters.h:15) */
+    int device;         /* CUDA device ordinal (parameters.h:76) */
+} rhmc_params;
+
+/* ------------------------------------------------------------------ lifecycle */
+const char *rhmc_last_error(void);
+/* Allocates the device-resident fields; replaces the per-trajectory cudaMalloc of
+ * cuda_init0/cuda_init1 (lib/Cuda/cuda_init.cu:5-109). */
+int rhmc_create(const rhmc_params *p, rhmc_ctx **out);
+int rhmc_destroy(rhmc_ctx *ctx);
+/* Issue subsequent work on a caller stream (cudaStream_t); NULL restores the context's own. */
+int rhmc_set_stream(rhmc_ctx *ctx, void *stream);
+int rhmc_sync(rhmc_ctx *ctx);
+/* Number of kernels this context has launched so far. */
+int rhmc_launch_count(const rhmc_ctx *ctx, long *count);
+
+/* ------------------------------------------------------------------ geometry */
+/* Neighbour table int[8V] (nnm mu=0..3 then nnp mu=0..3; make_shift_table,
+ * lib/Tools/Packer/packer.cc:415-439) and staggered phases int[4V] (init_geo,
+ * lib/Main/Geometry/geometry.cc:26-161), computed on the device into host buffers.
+ * Either pointer may be NULL. */
+int rhmc_geometry(rhmc_ctx *ctx, int *table, int *eta);
+
+/* ------------------------------------------------------------------ fields */
+/* Gauge field in the reference layout; replaces the gauge half of cuda_init0 / cuda_end
+ * (lib/Cuda/cuda_init.cu:5-58, 187-211) without the float hi/lo split. */
+int rhmc_set_gauge(rhmc_ctx *ctx, const double *u, int location);
+int rhmc_get_gauge(rhmc_ctx *ctx, double *u, int location);
+/* Momenta (traceless hermitian) and ipdot (traceless anti-hermitian) as full 3x3 matrices
+ * in the reference layout; stored internally as 8 reals per link.  Replaces the P/ipdot
+ * parts of cuda_init1 / cuda_end / cuda_get_momenta / cuda_put_momenta. */
+int rhmc_set_momenta(rhmc_ctx *ctx, const double *p, int location);
+int rhmc_get_momenta(rhmc_ctx *ctx, double *p, int location);
+int rhmc_set_ipdot(rhmc_ctx *ctx, const double *ip, int location);
+int rhmc_get_ipdot(rhmc_ctx *ctx, double *ip, int location);
+
+/* Spinor conversion between the reference layout (n consecutive complex[Vh][3]) and the
+ * internal device layout of format `fmt` precision.  `internal` is a device pointer. */
+int rhmc_spinor_to_internal(rhmc_ctx *ctx, int fmt, void *internal, const double *ref, int n, int location);
+int rhmc_spinor_from_internal(rhmc_ctx *ctx, int fmt, double *ref, const void *internal, int n, int location);
+
+/* ------------------------------------------------------------------ Dslash */
+/* out = D in onto parity `parity_out` (0: Deo, 1: Doe; lib/Action/fermionmatrix.cc:8-97,
+ * including the factor 1/2), for n right-hand sides sharing each link load.  in/out are
+ * internal-layout device spinors of the precision of `fmt`. */
+int rhmc_dslash(rhmc_ctx *ctx, int fmt, int parity_out, void *out, const void *in, int n);
+/* Reference-facing form of Deo/Doe: host spinors in the reference layout, FP64 links.
+ * Copies in, applies, copies out (used for the end-to-end measurement). */
+int rhmc_dslash_host(rhmc_ctx *ctx, int parity_out, double *out, const double *in);
+/* out = (M^dag M + shift) in on even sites = (mass^2 + shift) in - Deo Doe in
+ * (lib/Action/Inverter/inverter.cc:3, 206-216); internal-layout device spinors. */
+int rhmc_mdagm(rhmc_ctx *ctx, int fmt, void *out, const void *in, double shift, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RHMC_B200_H */

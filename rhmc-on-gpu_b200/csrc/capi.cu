@@ -1,0 +1,269 @@
+// capi.cu -- extern "C" surface of librhmc_b200 (declared in include/rhmc_b200.h):
+// context lifecycle, field I/O and the Dslash entry points.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "capi_util.h"
+#include "context.h"
+#include "kernels.h"
+
+namespace rhmc {
+
+static thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(RHMC_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Copies a caller buffer to the device if it lives on the host; returns the device pointer.
+int stage_in(rhmc_ctx *c, const char *slot, const void *src, size_t bytes, int location, const void **dev)
+{
+    if (location == RHMC_DEVICE) { *dev = src; return RHMC_OK; }
+    if (location != RHMC_HOST) return fail(RHMC_ERR_ARG, "location must be RHMC_HOST or RHMC_DEVICE");
+    void *p;
+    CK(c->ws.get(slot, bytes, &p));
+    CK(cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    *dev = p;
+    return RHMC_OK;
+}
+
+}  // namespace rhmc
+
+using namespace rhmc;
+
+extern "C" {
+
+const char *rhmc_last_error(void) { return g_err.c_str(); }
+
+int rhmc_create(const rhmc_params *p, rhmc_ctx **out)
+{
+    if (!p || !out) return fail(RHMC_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->nt <= 0 || (p->nx | p->ny | p->nz | p->nt) & 1)
+        return fail(RHMC_ERR_ARG, "lattice extents must be positive and even (got %d %d %d %d)", p->nx, p->ny, p->nz, p->nt);
+    const long V = (long)p->nx * p->ny * p->nz * p->nt;
+    if (V / 2 > 0x3fffffffL) return fail(RHMC_ERR_ARG, "lattice too large for 32-bit site indices");
+    CK(cudaSetDevice(p->device));
+    rhmc_ctx *c = new rhmc_ctx();
+    c->g.nx = p->nx; c->g.ny = p->ny; c->g.nz = p->nz; c->g.nt = p->nt;
+    c->g.Vh = (int)(V / 2);
+    c->g.antiperiodic_t = p->ferm_temp_bc == 0;
+    c->V = V; c->Vh = V / 2;
+    c->device = p->device;
+    c->mass = p->mass;
+    c->beta = p->beta;
+    c->U64 = nullptr; c->U64_12 = nullptr; c->U32_18 = nullptr; c->U32_12 = nullptr;
+    c->P = nullptr; c->IP = nullptr;
+    for (int i = 0; i < 4; i++) c->derived_valid[i] = false;
+    c->launches = 0;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    c->own_stream = true;
+    if (e == cudaSuccess) e = cudaMalloc(&c->U64, 8 * 9 * c->Vh * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&c->P, 8 * 8 * c->Vh * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&c->IP, 8 * 8 * c->Vh * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->U64, 0, 8 * 9 * c->Vh * sizeof(double2), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->P, 0, 8 * 8 * c->Vh * sizeof(double), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->IP, 0, 8 * 8 * c->Vh * sizeof(double), c->stream);
+    if (e != cudaSuccess) {
+        rhmc_destroy(c);
+        return cuda_fail(e, "rhmc_create");
+    }
+    *out = c;
+    return RHMC_OK;
+}
+
+int rhmc_destroy(rhmc_ctx *c)
+{
+    if (!c) return RHMC_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->U64); cudaFree(c->U64_12); cudaFree(c->U32_18); cudaFree(c->U32_12);
+    cudaFree(c->P); cudaFree(c->IP);
+    c->ws.release();
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return RHMC_OK;
+}
+
+int rhmc_set_stream(rhmc_ctx *c, void *stream)
+{
+    if (!c) return fail(RHMC_ERR_ARG, "null context");
+    if (stream) {
+        if (c->own_stream) { cudaStreamSynchronize(c->stream); cudaStreamDestroy(c->stream); }
+        c->stream = (cudaStream_t)stream;
+        c->own_stream = false;
+    } else if (!c->own_stream) {
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    return RHMC_OK;
+}
+
+int rhmc_sync(rhmc_ctx *c)
+{
+    if (!c) return fail(RHMC_ERR_ARG, "null context");
+    CK(cudaStreamSynchronize(c->stream));
+    return RHMC_OK;
+}
+
+int rhmc_launch_count(const rhmc_ctx *c, long *count)
+{
+    if (!c || !count) return fail(RHMC_ERR_ARG, "null argument");
+    *count = c->launches;
+    return RHMC_OK;
+}
+
+int rhmc_geometry(rhmc_ctx *c, int *table, int *eta)
+{
+    if (!c) return fail(RHMC_ERR_ARG, "null context");
+    void *dt = nullptr, *de = nullptr;
+    if (table) CK(c->ws.get("geom_table", 8 * c->V * sizeof(int), &dt));
+    if (eta) CK(c->ws.get("geom_eta", 4 * c->V * sizeof(int), &de));
+    launch_geometry(c, (int *)dt, (int *)de);
+    CK(cudaGetLastError());
+    if (table) CK(cudaMemcpyAsync(table, dt, 8 * c->V * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    if (eta) CK(cudaMemcpyAsync(eta, de, 4 * c->V * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return RHMC_OK;
+}
+
+int rhmc_set_gauge(rhmc_ctx *c, const double *u, int location)
+{
+    if (!c || !u) return fail(RHMC_ERR_ARG, "null argument");
+    const void *d;
+    int s = stage_in(c, "stage_gauge", u, 4 * c->V * 18 * sizeof(double), location, &d);
+    if (s) return s;
+    launch_gauge_from_ref(c, (const double *)d);
+    invalidate_links(c);
+    CK(cudaGetLastError());
+    return RHMC_OK;
+}
+
+int rhmc_get_gauge(rhmc_ctx *c, double *u, int location)
+{
+    if (!c || !u) return fail(RHMC_ERR_ARG, "null argument");
+    const size_t bytes = 4 * c->V * 18 * sizeof(double);
+    void *d = u;
+    if (location == RHMC_HOST) CK(c->ws.get("stage_gauge", bytes, &d));
+    launch_gauge_to_ref(c, (double *)d);
+    CK(cudaGetLastError());
+    if (location == RHMC_HOST) {
+        CK(cudaMemcpyAsync(u, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return RHMC_OK;
+}
+
+static int set_algebra(rhmc_ctx *c, double *A, const double *m, int location, int antiherm)
+{
+    if (!c || !m) return fail(RHMC_ERR_ARG, "null argument");
+    const void *d;
+    int s = stage_in(c, "stage_alg", m, 4 * c->V * 18 * sizeof(double), location, &d);
+    if (s) return s;
+    launch_algebra_from_ref(c, A, (const double *)d, antiherm);
+    CK(cudaGetLastError());
+    return RHMC_OK;
+}
+
+static int get_algebra(rhmc_ctx *c, const double *A, double *m, int location, int antiherm)
+{
+    if (!c || !m) return fail(RHMC_ERR_ARG, "null argument");
+    const size_t bytes = 4 * c->V * 18 * sizeof(double);
+    void *d = m;
+    if (location == RHMC_HOST) CK(c->ws.get("stage_alg", bytes, &d));
+    launch_algebra_to_ref(c, (double *)d, A, antiherm);
+    CK(cudaGetLastError());
+    if (location == RHMC_HOST) {
+        CK(cudaMemcpyAsync(m, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return RHMC_OK;
+}
+
+int rhmc_set_momenta(rhmc_ctx *c, const double *p, int location) { return set_algebra(c, c ? c->P : nullptr, p, location, 0); }
+int rhmc_get_momenta(rhmc_ctx *c, double *p, int location) { return get_algebra(c, c ? c->P : nullptr, p, location, 0); }
+int rhmc_set_ipdot(rhmc_ctx *c, const double *p, int location) { return set_algebra(c, c ? c->IP : nullptr, p, location, 1); }
+int rhmc_get_ipdot(rhmc_ctx *c, double *p, int location) { return get_algebra(c, c ? c->IP : nullptr, p, location, 1); }
+
+int rhmc_spinor_to_internal(rhmc_ctx *c, int fmt, void *internal, const double *ref, int n, int location)
+{
+    if (!c || !internal || !ref || n <= 0 || fmt < 0 || fmt > 3) return fail(RHMC_ERR_ARG, "bad argument");
+    const void *d;
+    int s = stage_in(c, "stage_spinor", ref, (size_t)n * c->Vh * 6 * sizeof(double), location, &d);
+    if (s) return s;
+    launch_spinor_to_internal(c, fmt_is_f64(fmt), internal, (const double *)d, n);
+    CK(cudaGetLastError());
+    return RHMC_OK;
+}
+
+int rhmc_spinor_from_internal(rhmc_ctx *c, int fmt, double *ref, const void *internal, int n, int location)
+{
+    if (!c || !internal || !ref || n <= 0 || fmt < 0 || fmt > 3) return fail(RHMC_ERR_ARG, "bad argument");
+    const size_t bytes = (size_t)n * c->Vh * 6 * sizeof(double);
+    void *d = ref;
+    if (location == RHMC_HOST) CK(c->ws.get("stage_spinor_out", bytes, &d));
+    launch_spinor_from_internal(c, fmt_is_f64(fmt), (double *)d, internal, n);
+    CK(cudaGetLastError());
+    if (location == RHMC_HOST) {
+        CK(cudaMemcpyAsync(ref, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return RHMC_OK;
+}
+
+int rhmc_dslash(rhmc_ctx *c, int fmt, int parity_out, void *out, const void *in, int n)
+{
+    if (!c || !out || !in || n <= 0 || (parity_out != 0 && parity_out != 1) || fmt < 0 || fmt > 3)
+        return fail(RHMC_ERR_ARG, "bad argument");
+    cudaError_t e = launch_dslash(c, fmt, parity_out, out, in, 3 * (size_t)c->Vh, n, nullptr, 0.0, 0.5, nullptr, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "rhmc_dslash");
+    return RHMC_OK;
+}
+
+int rhmc_dslash_host(rhmc_ctx *c, int parity_out, double *out, const double *in)
+{
+    if (!c || !out || !in || (parity_out != 0 && parity_out != 1)) return fail(RHMC_ERR_ARG, "bad argument");
+    const size_t bytes = (size_t)c->Vh * 6 * sizeof(double);
+    void *din, *dout, *iin, *iout;
+    CK(c->ws.get("dh_in", bytes, &din));
+    CK(c->ws.get("dh_out", bytes, &dout));
+    CK(c->ws.get("dh_iin", bytes, &iin));
+    CK(c->ws.get("dh_iout", bytes, &iout));
+    CK(cudaMemcpyAsync(din, in, bytes, cudaMemcpyHostToDevice, c->stream));
+    launch_spinor_to_internal(c, true, iin, (const double *)din, 1);
+    cudaError_t e = launch_dslash(c, RHMC_LINKS_F64_18, parity_out, iout, iin, 3 * (size_t)c->Vh, 1, nullptr, 0.0, 0.5, nullptr, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "rhmc_dslash_host");
+    launch_spinor_from_internal(c, true, (double *)dout, iout, 1);
+    CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return RHMC_OK;
+}
+
+int rhmc_mdagm(rhmc_ctx *c, int fmt, void *out, const void *in, double shift, int n)
+{
+    if (!c || !out || !in || n <= 0 || fmt < 0 || fmt > 3) return fail(RHMC_ERR_ARG, "bad argument");
+    const size_t es = fmt_is_f64(fmt) ? sizeof(double2) : sizeof(float2);
+    void *h;
+    CK(c->ws.get("mdagm_h", (size_t)n * 3 * c->Vh * es, &h));
+    cudaError_t e = launch_dslash(c, fmt, 1, h, in, 3 * (size_t)c->Vh, n, nullptr, 0.0, 0.5, nullptr, nullptr);
+    if (e == cudaSuccess)
+        e = launch_dslash(c, fmt, 0, out, h, 3 * (size_t)c->Vh, n, in, c->mass * c->mass + shift, -0.5, nullptr, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "rhmc_mdagm");
+    return RHMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// context.h -- the device-resident state behind one rhmc_ctx handle.
+//
+// The reference keeps its device state in file-scope globals that are reallocated every
+// trajectory (lib/Cuda/cuda_rhmc.cuh:73-79, lib/Cuda/cuda_init.cu:5-109) and mallocs solver
+// scratch on every call (lib/Cuda/cuda_inverter.cu:463,594).  Here every field lives in one
+// context for the lifetime of the handle; scratch is a grow-only named workspace.
+#pragma once
+#include <cuda_runtime.h>
+#include <map>
+#include <string>
+
+#include "rhmc_core.cuh"
+#include "../../include/rhmc_b200.h"
+
+namespace rhmc {
+
+struct Workspace {
+    std::map<std::string, std::pair<void *, size_t>> buf;
+    cudaError_t get(const std::string &name, size_t bytes, void **out)
+    {
+        auto it = buf.find(name);
+        if (it != buf.end() && it->second.second >= bytes) { *out = it->second.first; return cudaSuccess; }
+        if (it != buf.end()) { cudaFree(it->second.first); buf.erase(it); }
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+        if (e != cudaSuccess) return e;
+        buf[name] = std::make_pair(p, bytes);
+        *out = p;
+        return cudaSuccess;
+    }
+    void release()
+    {
+        for (auto &kv : buf) cudaFree(kv.second.first);
+        buf.clear();
+    }
+};
+
+}  // namespace rhmc
+
+struct rhmc_ctx {
+    rhmc::Geom g;
+    long V, Vh;
+    int device;
+    double mass, beta;
+    cudaStream_t stream;
+    bool own_stream;
+    // gauge field: FP64 18-real master ([mu][parity][9][Vh] double2) + derived formats
+    double2 *U64;
+    double2 *U64_12;
+    float4 *U32_18;
+    float4 *U32_12;
+    bool derived_valid[4];
+    // momenta and ipdot: FP64 algebra planes [mu][parity][8][Vh]
+    double *P;
+    double *IP;
+    rhmc::Workspace ws;
+    int launches;  // kernels launched by this context (counted by the host wrappers)
+};
+
+namespace rhmc {
+// link format accessor for kernels; ensures the derived copy is current
+cudaError_t links_f64_18(rhmc_ctx *c, L64_18 *lf);
+cudaError_t links_f64_12(rhmc_ctx *c, L64_12 *lf);
+cudaError_t links_f32_18(rhmc_ctx *c, L32_18 *lf);
+cudaError_t links_f32_12(rhmc_ctx *c, L32_12 *lf);
+void invalidate_links(rhmc_ctx *c);
+int grid_for(long n, int block);
+}  // namespace rhmc

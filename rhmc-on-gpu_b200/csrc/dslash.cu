@@ -1,0 +1,79 @@
+// dslash.cu -- instantiation and dispatch of the Dslash kernels (dslash.cuh).
+#include "context.h"
+#include "dslash.cuh"
+#include "kernels.h"
+
+namespace rhmc {
+
+bool fmt_is_f64(int fmt) { return fmt == RHMC_LINKS_F64_18 || fmt == RHMC_LINKS_F64_12; }
+
+int dslash_grid(rhmc_ctx *c) { return grid_for(c->Vh, DSLASH_BLOCK); }
+
+template <class LF, int NR>
+static void run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in, size_t stride, const void *y,
+                double alpha, double beta, double *partials)
+{
+    typedef typename LF::real R;
+    typedef typename SpinorT<R>::elem E;
+    DslashArgs<LF, NR> a;
+    a.g = c->g;
+    a.p_out = p_out;
+    a.links = lf;
+    a.in = (const E *)in;
+    a.out = (E *)out;
+    a.y = (const E *)y;
+    a.stride = stride;
+    a.alpha = (R)alpha;
+    a.beta = (R)beta;
+    a.partials = partials;
+    const int grid = dslash_grid(c);
+    if (y && partials) dslash_kernel<LF, NR, true, true><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
+    else if (y) dslash_kernel<LF, NR, true, false><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
+    else if (partials) dslash_kernel<LF, NR, false, true><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
+    else dslash_kernel<LF, NR, false, false><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
+    c->launches++;
+}
+
+template <class LF>
+static void run_n(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in, size_t stride, int n, const void *y,
+                  double alpha, double beta, double *partials)
+{
+    switch (n) {
+    case 1: run<LF, 1>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
+    case 2: run<LF, 2>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
+    case 3: run<LF, 3>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
+    case 4: run<LF, 4>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
+    case 8: run<LF, 8>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
+    default: {
+        // split into supported widths
+        typedef typename LF::real R;
+        typedef typename SpinorT<R>::elem E;
+        int done = 0;
+        while (done < n) {
+            int m = n - done >= 8 ? 8 : (n - done >= 4 ? 4 : n - done);
+            run_n<LF>(c, lf, p_out, (E *)out + done * stride, (const E *)in + done * stride, stride, m,
+                      y ? (const E *)y + done * stride : nullptr, alpha, beta, nullptr);
+            done += m;
+        }
+    }
+    }
+}
+
+cudaError_t launch_dslash(rhmc_ctx *c, int fmt, int p_out, void *out, const void *in, size_t stride, int n,
+                          const void *y, double alpha, double beta, double *partials, int *nblocks)
+{
+    if (partials && !(n == 1 || n == 2 || n == 3 || n == 4 || n == 8)) return cudaErrorInvalidValue;
+    if (nblocks) *nblocks = dslash_grid(c);
+    cudaError_t e = cudaSuccess;
+    switch (fmt) {
+    case RHMC_LINKS_F64_18: { L64_18 lf; e = links_f64_18(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
+    case RHMC_LINKS_F64_12: { L64_12 lf; e = links_f64_12(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
+    case RHMC_LINKS_F32_18: { L32_18 lf; e = links_f32_18(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
+    case RHMC_LINKS_F32_12: { L32_12 lf; e = links_f32_12(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
+    default: return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+}  // namespace rhmc

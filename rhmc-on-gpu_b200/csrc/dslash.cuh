@@ -1,0 +1,109 @@
+// dslash.cuh -- the even/odd staggered hopping term on sm_100a.
+//
+// Half-Dslash onto parity p (Deo for p = 0, Doe for p = 1; lib/Action/fermionmatrix.cc:8-97):
+//   (D in)(x) = 1/2 sum_mu [ U_mu(x) in(x+mu) - U_mu(x-mu)^dag in(x-mu) ]
+// with the staggered phases folded into the links.  One thread per output site; every
+// link is read exactly once per launch and shared by the NR right-hand sides the thread
+// carries; neighbour spinors come through the read-only path and are reused out of L2
+// (one parity of a 32^4 FP64 spinor is 25 MB, well inside the 126 MB L2).
+//
+// Epilogue: out = alpha*y + beta*(2 D in)/2, i.e. beta = +0.5 gives D, beta = -0.5 with
+// alpha = mass^2 + sigma and y = p gives the even-even (M^dag M + sigma) p from D_oe p
+// (lib/Action/Inverter/inverter.cc:206-216).  With RED the kernel also reduces, per RHS,
+// Re<y, out> and |out|^2 in FP64 into per-block partials (summed by the caller's
+// last-block step, so the order of summation is fixed and results are reproducible).
+#pragma once
+#include "rhmc_core.cuh"
+
+namespace rhmc {
+
+constexpr int DSLASH_BLOCK = 256;
+
+template <class LF, int NR>
+struct DslashArgs {
+    typedef typename LF::real R;
+    typedef typename SpinorT<R>::elem E;
+    Geom g;
+    int p_out;
+    LF links;
+    const E *in;        // NR spinors of parity 1-p_out, stride `stride` elements
+    E *out;             // NR spinors of parity p_out
+    const E *y;         // optional, parity p_out
+    size_t stride;      // elements between consecutive RHS (>= 3*Vh)
+    R alpha, beta;
+    double *partials;   // [gridDim.x][2*NR] when RED
+};
+
+template <class LF, int NR, bool HAS_Y, bool RED>
+__global__ void __launch_bounds__(DSLASH_BLOCK) dslash_kernel(DslashArgs<LF, NR> a)
+{
+    typedef typename LF::real R;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Vh = a.g.Vh;
+    double red[2 * NR > 0 ? 2 * NR : 1];
+#pragma unroll
+    for (int j = 0; j < 2 * NR; j++) red[j] = 0.0;
+
+    if (k < Vh) {
+        const Site s = site_of(a.g, a.p_out, k);
+        vec3<R> acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[r].c[c] = mk<R>(0, 0);
+#pragma unroll
+        for (int mu = 0; mu < 4; mu++) {
+            su3m<R> u;
+            const int kf = neighbour(a.g, s, mu, +1);
+            a.links.load(mu, a.p_out, k, u, eta_of(a.g, s, mu));
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                vec3<R> v = load_spinor<R>(a.in + r * a.stride, Vh, kf);
+                mv_acc(u, v, acc[r]);
+            }
+            const int kb = neighbour(a.g, s, mu, -1);
+            a.links.load(mu, 1 - a.p_out, kb, u, eta_back(a.g, s, mu));
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                vec3<R> v = load_spinor<R>(a.in + r * a.stride, Vh, kb);
+                mdv_sub(u, v, acc[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            vec3<R> o;
+            if (HAS_Y) {
+                vec3<R> yv = load_spinor<R>(a.y + r * a.stride, Vh, k);
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    o.c[c] = mk<R>(a.alpha * yv.c[c].re + a.beta * acc[r].c[c].re,
+                                   a.alpha * yv.c[c].im + a.beta * acc[r].c[c].im);
+                if (RED) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        red[2 * r] += (double)yv.c[c].re * (double)o.c[c].re + (double)yv.c[c].im * (double)o.c[c].im;
+                        red[2 * r + 1] += (double)o.c[c].re * (double)o.c[c].re + (double)o.c[c].im * (double)o.c[c].im;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; c++) o.c[c] = mk<R>(a.beta * acc[r].c[c].re, a.beta * acc[r].c[c].im);
+                if (RED) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++)
+                        red[2 * r + 1] += (double)o.c[c].re * (double)o.c[c].re + (double)o.c[c].im * (double)o.c[c].im;
+                }
+            }
+            store_spinor<R>(a.out + r * a.stride, Vh, k, o);
+        }
+    }
+    if (RED) {
+        __shared__ double smem[2 * NR * 32];
+        block_sum<2 * NR>(red, smem);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int j = 0; j < 2 * NR; j++) a.partials[(size_t)blockIdx.x * 2 * NR + j] = red[j];
+    }
+}
+
+}  // namespace rhmc

@@ -1,0 +1,292 @@
+// rhmc_core.cuh -- device-side building blocks shared by every kernel of librhmc_b200.
+//
+// Lattice: even/odd ordering of coppolachan/RHMC-on-GPU (lib/Main/Geometry/geometry.cc:5-11,86):
+// site (parity p, half index k) has lex = x + nx*(y + ny*(z + nz*t)) with k = lex/2.
+// Neighbours and staggered phases are computed from coordinates in the kernels instead of
+// being read from int tables (saves 32 B/site of HBM traffic per half-Dslash); the table
+// kernel in lattice.cu uses the same functions, so its bit-exact comparison with the
+// reference's make_shift_table (lib/Tools/Packer/packer.cc:415-439) covers the Dslash too.
+//
+// Field layouts in HBM (structure of arrays, one plane per complex element so that a warp
+// reads 32 consecutive sites per load instruction):
+//   links    [mu][parity][plane][Vh]  (planes per format below)
+//   spinor   [colour][Vh]             complex (double2 or float2); R right-hand sides are
+//                                      consecutive spinors (stride 3*Vh elements)
+//   algebra  [mu][parity][8][Vh]      reals: traceless (anti-)hermitian matrices
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rhmc {
+
+// ------------------------------------------------------------------ complex helpers
+template <typename R> struct cpx;
+template <> struct cpx<double> { double re, im; };
+template <> struct cpx<float> { float re, im; };
+
+template <typename R> __host__ __device__ __forceinline__ cpx<R> mk(R a, R b) { cpx<R> c; c.re = a; c.im = b; return c; }
+template <typename R> __device__ __forceinline__ cpx<R> operator+(cpx<R> a, cpx<R> b) { return mk<R>(a.re + b.re, a.im + b.im); }
+template <typename R> __device__ __forceinline__ cpx<R> operator-(cpx<R> a, cpx<R> b) { return mk<R>(a.re - b.re, a.im - b.im); }
+template <typename R> __device__ __forceinline__ cpx<R> operator*(cpx<R> a, cpx<R> b) { return mk<R>(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+template <typename R> __device__ __forceinline__ cpx<R> operator*(R s, cpx<R> a) { return mk<R>(s * a.re, s * a.im); }
+template <typename R> __device__ __forceinline__ cpx<R> conj(cpx<R> a) { return mk<R>(a.re, -a.im); }
+// a*b + c, a^* b + c
+template <typename R> __device__ __forceinline__ cpx<R> cmadd(cpx<R> a, cpx<R> b, cpx<R> c)
+{ return mk<R>(c.re + a.re * b.re - a.im * b.im, c.im + a.re * b.im + a.im * b.re); }
+template <typename R> __device__ __forceinline__ cpx<R> cjmadd(cpx<R> a, cpx<R> b, cpx<R> c)
+{ return mk<R>(c.re + a.re * b.re + a.im * b.im, c.im + a.re * b.im - a.im * b.re); }
+
+template <typename R> struct su3m { cpx<R> e[3][3]; };
+template <typename R> struct vec3 { cpx<R> c[3]; };
+
+// ------------------------------------------------------------------ lattice geometry
+struct Geom {
+    int nx, ny, nz, nt;
+    int Vh;          // sites per parity
+    int antiperiodic_t;  // 1: fermion phases flip on t = nt-1 (ferm_temp_bc == 0)
+};
+
+struct Site { int x, y, z, t; };
+
+// coordinates of (parity p, half index k)
+__host__ __device__ __forceinline__ Site site_of(const Geom &g, int p, int k)
+{
+    int lex2 = 2 * k;
+    int x0 = lex2 % g.nx;
+    int r = lex2 / g.nx;
+    Site s;
+    s.y = r % g.ny;
+    r /= g.ny;
+    s.z = r % g.nz;
+    s.t = r / g.nz;
+    s.x = x0 + ((p + x0 + s.y + s.z + s.t) & 1);
+    return s;
+}
+
+__host__ __device__ __forceinline__ int half_index(const Geom &g, int x, int y, int z, int t)
+{
+    return (x + g.nx * (y + g.ny * (z + g.nz * t))) >> 1;
+}
+
+// half index of the neighbour x + dir*mu (dir = +1/-1), periodic in every direction
+__host__ __device__ __forceinline__ int neighbour(const Geom &g, Site s, int mu, int dir)
+{
+    int x = s.x, y = s.y, z = s.z, t = s.t;
+    if (mu == 0) { x += dir; x = (x < 0) ? g.nx - 1 : (x >= g.nx ? 0 : x); }
+    else if (mu == 1) { y += dir; y = (y < 0) ? g.ny - 1 : (y >= g.ny ? 0 : y); }
+    else if (mu == 2) { z += dir; z = (z < 0) ? g.nz - 1 : (z >= g.nz ? 0 : z); }
+    else { t += dir; t = (t < 0) ? g.nt - 1 : (t >= g.nt ? 0 : t); }
+    return half_index(g, x, y, z, t);
+}
+
+// staggered phase eta_mu(x) (geometry.cc:107-153) with the antiperiodic time boundary
+__host__ __device__ __forceinline__ int eta_of(const Geom &g, Site s, int mu)
+{
+    int e;
+    if (mu == 0) e = 1;
+    else if (mu == 1) e = 1 - 2 * (s.x & 1);
+    else if (mu == 2) e = 1 - 2 * ((s.x + s.y) & 1);
+    else {
+        e = 1 - 2 * ((s.x + s.y + s.z) & 1);
+        if (g.antiperiodic_t && s.t == g.nt - 1) e = -e;
+    }
+    return e;
+}
+
+// eta of the link U_mu(x - mu): equal to eta_mu(x) except for the time boundary flip
+__host__ __device__ __forceinline__ int eta_back(const Geom &g, Site s, int mu)
+{
+    int e;
+    if (mu == 0) e = 1;
+    else if (mu == 1) e = 1 - 2 * (s.x & 1);
+    else if (mu == 2) e = 1 - 2 * ((s.x + s.y) & 1);
+    else {
+        e = 1 - 2 * ((s.x + s.y + s.z) & 1);
+        if (g.antiperiodic_t && s.t == 0) e = -e;
+    }
+    return e;
+}
+
+// ------------------------------------------------------------------ link formats
+// Row 2 is reconstructed as eta * conj(row0 x row1), the relation Conf::unitarize_with_eta
+// (lib/Main/Conf/conf.cc:235-251) leaves in every stored link; the reference GPU code
+// reconstructs the same way (lib/Cuda/cuda_rhmc.cuh:32-45).
+template <typename R>
+__device__ __forceinline__ void reconstruct_row2(su3m<R> &u, R eta)
+{
+    cpx<R> a = u.e[0][1] * u.e[1][2] - u.e[0][2] * u.e[1][1];
+    cpx<R> b = u.e[0][2] * u.e[1][0] - u.e[0][0] * u.e[1][2];
+    cpx<R> c = u.e[0][0] * u.e[1][1] - u.e[0][1] * u.e[1][0];
+    u.e[2][0] = mk<R>(eta * a.re, -eta * a.im);
+    u.e[2][1] = mk<R>(eta * b.re, -eta * b.im);
+    u.e[2][2] = mk<R>(eta * c.re, -eta * c.im);
+}
+
+// FP64, 18 reals: 9 double2 planes
+struct L64_18 {
+    typedef double real;
+    static constexpr int planes = 9;
+    static constexpr int reals = 18;
+    static constexpr int bytes = 144;
+    const double2 *__restrict__ p;
+    int Vh;
+    __device__ __forceinline__ void load(int mu, int par, int k, su3m<double> &u, int) const
+    {
+        const double2 *b = p + (size_t)((mu * 2 + par) * 9) * Vh + k;
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            double2 v = __ldg(b + (size_t)e * Vh);
+            u.e[e / 3][e % 3] = mk<double>(v.x, v.y);
+        }
+    }
+};
+
+// FP64, 12 reals: 6 double2 planes, row 2 reconstructed
+struct L64_12 {
+    typedef double real;
+    static constexpr int planes = 6;
+    static constexpr int reals = 12;
+    static constexpr int bytes = 96;
+    const double2 *__restrict__ p;
+    int Vh;
+    __device__ __forceinline__ void load(int mu, int par, int k, su3m<double> &u, int eta) const
+    {
+        const double2 *b = p + (size_t)((mu * 2 + par) * 6) * Vh + k;
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            double2 v = __ldg(b + (size_t)e * Vh);
+            u.e[e / 3][e % 3] = mk<double>(v.x, v.y);
+        }
+        reconstruct_row2<double>(u, (double)eta);
+    }
+};
+
+// FP32, 18 reals: 4 float4 planes + 1 float2 plane (the float2 planes follow all float4 ones)
+struct L32_18 {
+    typedef float real;
+    static constexpr int planes = 5;
+    static constexpr int reals = 18;
+    static constexpr int bytes = 72;
+    const float4 *__restrict__ p;
+    int Vh;
+    __device__ __forceinline__ void load(int mu, int par, int k, su3m<float> &u, int) const
+    {
+        const float4 *b = p + (size_t)((mu * 2 + par) * 4) * Vh + k;
+        float4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh), a3 = __ldg(b + 3 * (size_t)Vh);
+        const float2 *q = reinterpret_cast<const float2 *>(p + (size_t)32 * Vh) + (size_t)(mu * 2 + par) * Vh + k;
+        float2 a4 = __ldg(q);
+        u.e[0][0] = mk<float>(a0.x, a0.y); u.e[0][1] = mk<float>(a0.z, a0.w);
+        u.e[0][2] = mk<float>(a1.x, a1.y); u.e[1][0] = mk<float>(a1.z, a1.w);
+        u.e[1][1] = mk<float>(a2.x, a2.y); u.e[1][2] = mk<float>(a2.z, a2.w);
+        u.e[2][0] = mk<float>(a3.x, a3.y); u.e[2][1] = mk<float>(a3.z, a3.w);
+        u.e[2][2] = mk<float>(a4.x, a4.y);
+    }
+};
+
+// FP32, 12 reals: 3 float4 planes, row 2 reconstructed
+struct L32_12 {
+    typedef float real;
+    static constexpr int planes = 3;
+    static constexpr int reals = 12;
+    static constexpr int bytes = 48;
+    const float4 *__restrict__ p;
+    int Vh;
+    __device__ __forceinline__ void load(int mu, int par, int k, su3m<float> &u, int eta) const
+    {
+        const float4 *b = p + (size_t)((mu * 2 + par) * 3) * Vh + k;
+        float4 a0 = __ldg(b), a1 = __ldg(b + Vh), a2 = __ldg(b + 2 * (size_t)Vh);
+        u.e[0][0] = mk<float>(a0.x, a0.y); u.e[0][1] = mk<float>(a0.z, a0.w);
+        u.e[0][2] = mk<float>(a1.x, a1.y); u.e[1][0] = mk<float>(a1.z, a1.w);
+        u.e[1][1] = mk<float>(a2.x, a2.y); u.e[1][2] = mk<float>(a2.z, a2.w);
+        reconstruct_row2<float>(u, (float)eta);
+    }
+};
+
+// ------------------------------------------------------------------ spinor formats
+template <typename R> struct SpinorT;
+template <> struct SpinorT<double> { typedef double2 elem; };
+template <> struct SpinorT<float> { typedef float2 elem; };
+
+template <typename R>
+__device__ __forceinline__ vec3<R> load_spinor(const typename SpinorT<R>::elem *__restrict__ v, int Vh, int k)
+{
+    vec3<R> r;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        typename SpinorT<R>::elem a = __ldg(v + (size_t)c * Vh + k);
+        r.c[c] = mk<R>(a.x, a.y);
+    }
+    return r;
+}
+
+template <typename R>
+__device__ __forceinline__ void store_spinor(typename SpinorT<R>::elem *v, int Vh, int k, const vec3<R> &r)
+{
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        typename SpinorT<R>::elem a;
+        a.x = r.c[c].re;
+        a.y = r.c[c].im;
+        v[(size_t)c * Vh + k] = a;
+    }
+}
+
+// ------------------------------------------------------------------ SU(3) x vector
+// acc += U v
+template <typename R>
+__device__ __forceinline__ void mv_acc(const su3m<R> &u, const vec3<R> &v, vec3<R> &acc)
+{
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        cpx<R> s = acc.c[i];
+        s = cmadd(u.e[i][0], v.c[0], s);
+        s = cmadd(u.e[i][1], v.c[1], s);
+        s = cmadd(u.e[i][2], v.c[2], s);
+        acc.c[i] = s;
+    }
+}
+
+// acc -= U^dag v
+template <typename R>
+__device__ __forceinline__ void mdv_sub(const su3m<R> &u, const vec3<R> &v, vec3<R> &acc)
+{
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        cpx<R> s = mk<R>(0, 0);
+        s = cjmadd(u.e[0][i], v.c[0], s);
+        s = cjmadd(u.e[1][i], v.c[1], s);
+        s = cjmadd(u.e[2][i], v.c[2], s);
+        acc.c[i] = acc.c[i] - s;
+    }
+}
+
+// ------------------------------------------------------------------ reductions
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of N values per thread; result valid in thread 0.  smem: N*32 doubles.
+template <int N>
+__device__ __forceinline__ void block_sum(double (&v)[N], double *smem)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int j = 0; j < N; j++) v[j] = warp_sum(v[j]);
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < N; j++) smem[j * 32 + wid] = v[j];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            double a = (lane < nw) ? smem[j * 32 + lane] : 0.0;
+            v[j] = warp_sum(a);
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace rhmc

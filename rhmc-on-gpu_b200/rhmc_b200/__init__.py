@@ -1,0 +1,176 @@
+"""Python front-end of librhmc_b200 (ctypes over the C ABI declared in include/rhmc_b200.h).
+
+The library is the product; this module only loads it and forwards calls.  Device buffers
+are passed as raw pointers (``int``) so any allocator works; the tests and bench use torch
+tensors for device memory.  There is no CPU fallback: if the shared library is missing the
+import of ``lib()`` raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIBPATH = os.path.join(PKG, "librhmc_b200.so")
+
+RHMC_OK = 0
+LINKS_F64_18, LINKS_F64_12, LINKS_F32_18, LINKS_F32_12 = 0, 1, 2, 3
+FMT_NAMES = {LINKS_F64_18: "f64_18", LINKS_F64_12: "f64_12", LINKS_F32_18: "f32_18", LINKS_F32_12: "f32_12"}
+HOST, DEVICE = 0, 1
+
+_lib = None
+
+
+class RhmcError(RuntimeError):
+    pass
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("nt", ctypes.c_int),
+                ("ferm_temp_bc", ctypes.c_int), ("mass", ctypes.c_double), ("beta", ctypes.c_double),
+                ("device", ctypes.c_int)]
+
+
+def build(force=False):
+    """Compile the library in-tree with the package Makefile (nvcc, sm_100a)."""
+    import subprocess
+    cmd = ["make", "-C", PKG, "-j8"]
+    if force:
+        subprocess.check_call(["make", "-C", PKG, "clean"])
+    subprocess.check_call(cmd)
+    return LIBPATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise RhmcError("librhmc_b200.so not built (run __graft_entry__.build())")
+        _lib = ctypes.CDLL(LIBPATH)
+        _lib.rhmc_last_error.restype = ctypes.c_char_p
+    return _lib
+
+
+def _check(rc):
+    if rc != RHMC_OK:
+        raise RhmcError("rhmc error %d: %s" % (rc, lib().rhmc_last_error().decode()))
+    return rc
+
+
+def _vp(x):
+    """Pointer argument: int (device address), numpy array (host), None."""
+    if x is None:
+        return ctypes.c_void_p(None)
+    if isinstance(x, int):
+        return ctypes.c_void_p(x)
+    if isinstance(x, np.ndarray):
+        assert x.flags.c_contiguous
+        return ctypes.c_void_p(x.ctypes.data)
+    if hasattr(x, "data_ptr"):
+        return ctypes.c_void_p(x.data_ptr())
+    raise TypeError(type(x))
+
+
+def _loc(x):
+    return HOST if isinstance(x, np.ndarray) else DEVICE
+
+
+class Context:
+    """One rhmc_ctx: a lattice with device-resident gauge field, momenta and ipdot."""
+
+    def __init__(self, dims, mass=0.1, beta=5.5, ferm_temp_bc=0, device=0):
+        self.dims = tuple(int(d) for d in dims)
+        self.V = int(np.prod(self.dims))
+        self.Vh = self.V // 2
+        self.mass, self.beta = mass, beta
+        p = Params(*self.dims, ferm_temp_bc, mass, beta, device)
+        h = ctypes.c_void_p()
+        _check(lib().rhmc_create(ctypes.byref(p), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().rhmc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def call(self, name, *args):
+        conv = []
+        for a in args:
+            if isinstance(a, float):
+                conv.append(ctypes.c_double(a))
+            elif isinstance(a, (np.ndarray,)) or hasattr(a, "data_ptr") or a is None:
+                conv.append(_vp(a))
+            elif isinstance(a, ctypes._SimpleCData) or isinstance(a, ctypes.Array) or hasattr(a, "_obj"):
+                conv.append(a)
+            elif isinstance(a, int):
+                conv.append(ctypes.c_int(a))
+            else:
+                conv.append(a)
+        return _check(getattr(lib(), name)(self.h, *conv))
+
+    def set_stream(self, stream_ptr):
+        _check(lib().rhmc_set_stream(self.h, ctypes.c_void_p(stream_ptr)))
+
+    def sync(self):
+        self.call("rhmc_sync")
+
+    def launch_count(self):
+        n = ctypes.c_long()
+        self.call("rhmc_launch_count", ctypes.byref(n))
+        return n.value
+
+    def geometry(self):
+        t = np.zeros(8 * self.V, np.int32)
+        e = np.zeros(4 * self.V, np.int32)
+        self.call("rhmc_geometry", t, e)
+        return t, e
+
+    # fields: numpy (host) or torch (device) in the reference layout
+    def set_gauge(self, u):
+        self.call("rhmc_set_gauge", u, _loc(u))
+
+    def get_gauge(self, out=None):
+        if out is None:
+            out = np.zeros((4 * self.V, 3, 3), np.complex128)
+        self.call("rhmc_get_gauge", out, _loc(out))
+        return out
+
+    def set_momenta(self, p):
+        self.call("rhmc_set_momenta", p, _loc(p))
+
+    def get_momenta(self, out=None):
+        if out is None:
+            out = np.zeros((4 * self.V, 3, 3), np.complex128)
+        self.call("rhmc_get_momenta", out, _loc(out))
+        return out
+
+    def set_ipdot(self, p):
+        self.call("rhmc_set_ipdot", p, _loc(p))
+
+    def get_ipdot(self, out=None):
+        if out is None:
+            out = np.zeros((4 * self.V, 3, 3), np.complex128)
+        self.call("rhmc_get_ipdot", out, _loc(out))
+        return out
+
+    def spinor_to_internal(self, fmt, internal, ref, n=1):
+        self.call("rhmc_spinor_to_internal", fmt, internal, ref, n, _loc(ref))
+
+    def spinor_from_internal(self, fmt, ref, internal, n=1):
+        self.call("rhmc_spinor_from_internal", fmt, ref, internal, n, _loc(ref))
+
+    def dslash(self, fmt, parity_out, out, inp, n=1):
+        self.call("rhmc_dslash", fmt, parity_out, out, inp, n)
+
+    def dslash_host(self, parity_out, out, inp):
+        self.call("rhmc_dslash_host", parity_out, out, inp)
+
+    def mdagm(self, fmt, out, inp, shift=0.0, n=1):
+        self.call("rhmc_mdagm", fmt, out, inp, float(shift), n)
