@@ -107,6 +107,51 @@ int rhmc_dslash_host(rhmc_ctx *ctx, int parity_out, double *out, const double *i
  * (lib/Action/Inverter/inverter.cc:3, 206-216); internal-layout device spinors. */
 int rhmc_mdagm(rhmc_ctx *ctx, int fmt, void *out, const void *in, double shift, int n);
 
+/* ------------------------------------------------------------------ multi-shift CG */
+enum {
+    RHMC_MSOLVE_FP64 = 0,  /* the reference algorithm in FP64 (multips_shifted_invert,
+                              lib/Action/Inverter/inverter.cc:142-339): base operator M^dag M,
+                              shift frozen when sqrt(|r|^2 zeta^2) < residual */
+    RHMC_MSOLVE_MIXED = 1, /* FP32 multi-shift on the smallest pole, all RHS batched, then FP32
+                              CG per system with FP64 reliable updates until every FP64 true
+                              residual |b - (M^dag M + sigma_i) x_i| <= residual */
+    RHMC_MSOLVE_FP32 = 2   /* the reference algorithm with FP32 links and vectors (its
+                              single-precision path, lib/Cuda/cuda_inverter.cu:647-857, used
+                              when residual >= 1e-4, cu_inverter.cc:45-60); FP64 scalars */
+};
+
+typedef struct {
+    int nshift;            /* number of poles, 1..32 (max_approx_order, include/global_const.h:11) */
+    const double *shifts; /* sigma_i >= 0: the rescaled RA_b (rationalapprox.cc:162-170) */
+    int nrhs;              /* right-hand sides (pseudofermions) solved together */
+    double residual;       /* absolute stopping residual (residue_metro / residue_md, parameters.h:68,73) */
+    int max_iter;          /* iteration cap (max_cg, parameters.h:57) */
+    int mode;              /* RHMC_MSOLVE_* */
+    int fmt;               /* link format: FP64 ones for RHMC_MSOLVE_FP64, FP32 ones for RHMC_MSOLVE_MIXED */
+    double tol_phase_a;    /* mixed mode: relative residual of the FP32 multi-shift phase (0: 3e-6) */
+} rhmc_msolve_params;
+
+typedef struct {
+    int status;            /* RHMC_OK or the error returned */
+    int iters[8];          /* multi-shift iterations per RHS (first 8) */
+    long refine_iters;     /* mixed mode: batched refinement iterations (sum over batches) */
+    int reliable_updates;  /* mixed mode: FP64 residual recomputations */
+    double seconds;        /* wall time of the call */
+} rhmc_msolve_info;
+
+/* (M^dag M + sigma_i) x_{r,i} = b_r for every shift i and RHS r (cuda_shifted_inverter /
+ * cuda_shifted_inverter_d, lib/Cuda/cuda_inverter.cu:647-857, cuda_inverter_d.cu:752-968,
+ * called per pseudofermion by cu_multips_shifted_invert, lib/Action/Inverter/cu_inverter.cc:21-72).
+ * b: nrhs FP64 internal spinors (device); x: nrhs*nshift FP64 internal spinors, RHS-major
+ * (the ShiftMultiFermion order [no_ps][order][sizeh], lib/Action/fermions.h:114).
+ * Returns RHMC_ERR_MAXITER instead of the reference's exit(1) at max_cg. */
+int rhmc_msolve(rhmc_ctx *ctx, const rhmc_msolve_params *p, double *x, const double *b, rhmc_msolve_info *info);
+/* Same with host arrays in the reference layout: b complex[nrhs][Vh][3], x complex[nrhs][nshift][Vh][3]. */
+int rhmc_msolve_host(rhmc_ctx *ctx, const rhmc_msolve_params *p, double *x, const double *b, rhmc_msolve_info *info);
+/* |b_r - (M^dag M + sigma_i) x_{r,i}| in FP64 for every (r, i); out: host double[nrhs][nshift].
+ * The check of inverter.cc:306-338 / cu_inverter.cc:79-120 without the debug build. */
+int rhmc_true_residuals(rhmc_ctx *ctx, int nshift, const double *shifts, int nrhs, const double *x, const double *b, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,7 +70,13 @@ int rhmc_create(const rhmc_params *p, rhmc_ctx **out)
     c->P = nullptr; c->IP = nullptr;
     for (int i = 0; i < 4; i++) c->derived_valid[i] = false;
     c->launches = 0;
+    c->hflags = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&c->hflags, 256, cudaHostAllocDefault);
+    c->aux = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     c->own_stream = true;
     if (e == cudaSuccess) e = cudaMalloc(&c->U64, 8 * 9 * c->Vh * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&c->P, 8 * 8 * c->Vh * sizeof(double));
@@ -94,6 +100,12 @@ int rhmc_destroy(rhmc_ctx *c)
     cudaFree(c->U64); cudaFree(c->U64_12); cudaFree(c->U32_18); cudaFree(c->U32_12);
     cudaFree(c->P); cudaFree(c->IP);
     c->ws.release();
+    if (c->hflags) cudaFreeHost(c->hflags);
+    if (c->aux) {
+        cudaStreamDestroy(c->aux);
+        cudaEventDestroy(c->ev_fork);
+        cudaEventDestroy(c->ev_join);
+    }
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return RHMC_OK;

@@ -54,7 +54,12 @@ struct rhmc_ctx {
     double *P;
     double *IP;
     rhmc::Workspace ws;
-    int launches;  // kernels launched by this context (counted by the host wrappers)
+    int *hflags;   // pinned host words for polling device-side solver flags
+    // graph-captured solver loops run on this stream, ordered against `stream` by events
+    // (capture is not possible on the legacy default stream a caller may have installed)
+    cudaStream_t aux;
+    cudaEvent_t ev_fork, ev_join;
+    long launches;  // kernels launched by this context (counted by the host wrappers)
 };
 
 namespace rhmc {
@@ -65,4 +70,20 @@ cudaError_t links_f32_18(rhmc_ctx *c, L32_18 *lf);
 cudaError_t links_f32_12(rhmc_ctx *c, L32_12 *lf);
 void invalidate_links(rhmc_ctx *c);
 int grid_for(long n, int block);
+
+// Work issued on c->aux between the constructor and the destructor is ordered after
+// everything already on c->stream and before anything issued on it later.
+struct AuxScope {
+    rhmc_ctx *c;
+    explicit AuxScope(rhmc_ctx *cc) : c(cc)
+    {
+        cudaEventRecord(c->ev_fork, c->stream);
+        cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
+    }
+    ~AuxScope()
+    {
+        cudaEventRecord(c->ev_join, c->aux);
+        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    }
+};
 }  // namespace rhmc

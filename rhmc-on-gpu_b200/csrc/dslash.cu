@@ -25,12 +25,16 @@ static void run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in,
     a.stride = stride;
     a.alpha = (R)alpha;
     a.beta = (R)beta;
+    a.use_alphas = 0;
+    for (int r = 0; r < NR; r++) a.alphas[r] = (R)alpha;
     a.partials = partials;
+    a.ticket = nullptr;
+    a.stop = nullptr;
+    a.stop_set = nullptr;
+    a.run_if = nullptr;
     const int grid = dslash_grid(c);
-    if (y && partials) dslash_kernel<LF, NR, true, true><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
-    else if (y) dslash_kernel<LF, NR, true, false><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
-    else if (partials) dslash_kernel<LF, NR, false, true><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
-    else dslash_kernel<LF, NR, false, false><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
+    if (y) dslash_kernel<LF, NR, true, false, NoFin><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
+    else dslash_kernel<LF, NR, false, false, NoFin><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
     c->launches++;
 }
 
@@ -62,7 +66,7 @@ static void run_n(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *i
 cudaError_t launch_dslash(rhmc_ctx *c, int fmt, int p_out, void *out, const void *in, size_t stride, int n,
                           const void *y, double alpha, double beta, double *partials, int *nblocks)
 {
-    if (partials && !(n == 1 || n == 2 || n == 3 || n == 4 || n == 8)) return cudaErrorInvalidValue;
+    if (partials) return cudaErrorInvalidValue;  // reductions go through the solver's own launches
     if (nblocks) *nblocks = dslash_grid(c);
     cudaError_t e = cudaSuccess;
     switch (fmt) {

@@ -19,7 +19,7 @@ namespace rhmc {
 
 constexpr int DSLASH_BLOCK = 256;
 
-template <class LF, int NR>
+template <class LF, int NR, class FIN = NoFin>
 struct DslashArgs {
     typedef typename LF::real R;
     typedef typename SpinorT<R>::elem E;
@@ -31,13 +31,25 @@ struct DslashArgs {
     const E *y;         // optional, parity p_out
     size_t stride;      // elements between consecutive RHS (>= 3*Vh)
     R alpha, beta;
+    R alphas[NR];       // per-RHS alpha when use_alphas (shifted systems batched together)
+    int use_alphas;
     double *partials;   // [gridDim.x][2*NR] when RED
+    unsigned *ticket;   // last-block counter when RED (fin() runs on the totals)
+    FIN fin;
+    const int *stop;    // optional: skip the launch when *stop != 0 ...
+    int *stop_set;      // ... and then set *stop_set = 1 (solver loop control)
+    const int *run_if;  // optional: skip the launch when *run_if == 0
 };
 
-template <class LF, int NR, bool HAS_Y, bool RED>
-__global__ void __launch_bounds__(DSLASH_BLOCK) dslash_kernel(DslashArgs<LF, NR> a)
+template <class LF, int NR, bool HAS_Y, bool RED, class FIN>
+__global__ void __launch_bounds__(DSLASH_BLOCK) dslash_kernel(DslashArgs<LF, NR, FIN> a)
 {
     typedef typename LF::real R;
+    if (a.stop && *(volatile const int *)a.stop) {
+        if (a.stop_set && blockIdx.x == 0 && threadIdx.x == 0) *a.stop_set = 1;
+        return;
+    }
+    if (a.run_if && *(volatile const int *)a.run_if == 0) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int Vh = a.g.Vh;
     double red[2 * NR > 0 ? 2 * NR : 1];
@@ -74,10 +86,11 @@ __global__ void __launch_bounds__(DSLASH_BLOCK) dslash_kernel(DslashArgs<LF, NR>
             vec3<R> o;
             if (HAS_Y) {
                 vec3<R> yv = load_spinor<R>(a.y + r * a.stride, Vh, k);
+                const R al = a.use_alphas ? a.alphas[r] : a.alpha;
 #pragma unroll
                 for (int c = 0; c < 3; c++)
-                    o.c[c] = mk<R>(a.alpha * yv.c[c].re + a.beta * acc[r].c[c].re,
-                                   a.alpha * yv.c[c].im + a.beta * acc[r].c[c].im);
+                    o.c[c] = mk<R>(al * yv.c[c].re + a.beta * acc[r].c[c].re,
+                                   al * yv.c[c].im + a.beta * acc[r].c[c].im);
                 if (RED) {
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
@@ -97,13 +110,7 @@ __global__ void __launch_bounds__(DSLASH_BLOCK) dslash_kernel(DslashArgs<LF, NR>
             store_spinor<R>(a.out + r * a.stride, Vh, k, o);
         }
     }
-    if (RED) {
-        __shared__ double smem[2 * NR * 32];
-        block_sum<2 * NR>(red, smem);
-        if (threadIdx.x == 0)
-#pragma unroll
-            for (int j = 0; j < 2 * NR; j++) a.partials[(size_t)blockIdx.x * 2 * NR + j] = red[j];
-    }
+    if (RED) reduce_finalize<2 * NR>(red, a.partials, a.ticket, a.fin);
 }
 
 }  // namespace rhmc

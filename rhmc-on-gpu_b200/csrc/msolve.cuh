@@ -1,0 +1,311 @@
+// msolve.cuh -- multi-shift conjugate gradient on (M^dag M + sigma_i) x_i = b over even sites.
+//
+// Algorithm: Jegerlehner's multi-shift CG (hep-lat/9612014) exactly as the reference's CPU
+// solver runs it (multips_shifted_invert, lib/Action/Inverter/inverter.cc:142-299): x_i = 0,
+// r = p = p_i = b; per iteration
+//   s = (M^dag M + sigma_0) p, alpha = Re<p,s>, omega = -delta/alpha
+//   zeta'''_i = zeta_i zeta''_i omega_prev / (omega gamma (zeta_i - zeta''_i)
+//                                               + zeta_i omega_prev (1 - sigma_i omega))
+//   omega_i = omega zeta'''_i / zeta''_i ;  x_i -= omega_i p_i
+//   r += omega s, lambda = |r|^2, gamma = lambda/delta, p = r + gamma p
+//   gamma_i = gamma zeta'''_i omega_i / (zeta''_i omega) ; p_i = zeta'''_i r + gamma_i p_i
+//   freeze shift i when sqrt(delta zeta''_i^2) < tgt_i (lagged residual, as inverter.cc:275-279)
+// stopping when sqrt(lambda) <= res (inverter.cc:287), when every shift is frozen (the GPU
+// solver's criterion, cuda_inverter.cu:777-785) or at max_iter.  sigma_0 is the base shift
+// (0 in the reference; the mixed solver uses the smallest pole) and sigma_i are relative to it.
+//
+// Kernel sequence per iteration (one CUDA graph replays a chunk of iterations):
+//   K1 D_oe:    h = D_oe p                                   (Dslash, NR right-hand sides)
+//   K2 D_eo:    s = (m^2+sigma_0) p - D_eo h, Re<p,s>        (Dslash epilogue + FP64 reduction;
+//               the last block computes omega, zeta''', omega_i for every RHS)
+//   K3 resid:   r += omega s, |r|^2                          (last block: gamma, gamma_i, freezing,
+//               convergence, stop flag)
+//   K4 update:  p = r + gamma p; x_i -= omega_i p_i; p_i = zeta''' r + gamma_i p_i
+// Scalars live in device memory (MSState) and never leave the GPU during the solve; the host
+// only polls the stop flag between graph replays.
+#pragma once
+#include "dslash.cuh"
+
+namespace rhmc {
+
+constexpr int MS_MAX_SHIFT = 32;
+constexpr int MS_MAX_RHS = 8;
+constexpr int VEC_BLOCK = 256;
+
+struct MSRhs {
+    double delta, omega, omega_prev, gamma, lambda, alpha, b2;
+    int iter;          // iterations performed
+    int running;       // this iteration updates the RHS
+    int running_next;  // still running after this iteration
+    double zeta_i[MS_MAX_SHIFT], zeta_ii[MS_MAX_SHIFT], zeta_iii[MS_MAX_SHIFT];
+    double omegas[MS_MAX_SHIFT], gammas[MS_MAX_SHIFT];
+    int active[MS_MAX_SHIFT];       // shift updated in this iteration
+    int active_next[MS_MAX_SHIFT];  // after the freezing test
+};
+
+struct MSState {
+    int stop;     // every RHS finished: K1-K3 skip
+    int stop_k4;  // set by the first skipped K1 so that K4 skips from the next iteration on
+    int status;   // 0 ok, 1 iteration cap, 2 non-finite reduction
+    int nshift, nrhs, max_iter;
+    int stop_on_frozen;             // also stop when every shift is frozen
+    double res;                     // base residual target: stop when sqrt(lambda) <= res
+    double tgt[MS_MAX_SHIFT];       // freezing threshold for sqrt(delta zeta''^2)
+    double shift[MS_MAX_SHIFT];     // sigma_i - sigma_0
+    MSRhs rhs[MS_MAX_RHS];
+};
+
+// ------------------------------------------------------------------ last-block scalar steps
+struct FinInit {
+    MSState *st;
+    __device__ void operator()(const double *tot) const
+    {
+        for (int r = 0; r < st->nrhs; r++) {
+            MSRhs &q = st->rhs[r];
+            q.b2 = tot[r];
+            q.delta = tot[r];
+            q.omega = 1.0;
+            q.omega_prev = 1.0;
+            q.gamma = 0.0;
+            q.lambda = tot[r];
+            q.alpha = 0.0;
+            q.iter = 0;
+            q.running = 1;
+            q.running_next = (tot[r] > 0.0) ? 1 : 0;  // b == 0: x = 0 is exact
+            if (!isfinite(tot[r])) {
+                st->status = 2;
+                q.running_next = 0;
+            }
+            for (int i = 0; i < st->nshift; i++) {
+                q.zeta_i[i] = 1.0;
+                q.zeta_ii[i] = 1.0;
+                q.zeta_iii[i] = 1.0;
+                q.omegas[i] = 0.0;
+                q.gammas[i] = 0.0;
+                q.active[i] = 1;
+                q.active_next[i] = 1;
+            }
+        }
+        st->stop = 0;
+        st->stop_k4 = 0;
+        int any = 0;
+        for (int r = 0; r < st->nrhs; r++) any |= st->rhs[r].running_next;
+        if (!any) st->stop = 1;
+    }
+};
+
+template <int NR>
+struct FinAlpha {
+    MSState *st;
+    __device__ void operator()(const double *tot) const
+    {
+        for (int r = 0; r < NR; r++) {
+            MSRhs &q = st->rhs[r];
+            q.running = q.running_next;
+            if (!q.running) continue;
+            for (int i = 0; i < st->nshift; i++) q.active[i] = q.active_next[i];
+            q.alpha = tot[2 * r];
+            if (!isfinite(q.alpha) || q.alpha == 0.0) {
+                st->status = 2;
+                st->stop = 1;
+                q.running = 0;
+                q.running_next = 0;
+                continue;
+            }
+            q.omega_prev = q.omega;
+            q.omega = -q.delta / q.alpha;
+            for (int i = 0; i < st->nshift; i++) {
+                if (!q.active[i]) continue;
+                const double zi = q.zeta_i[i], zii = q.zeta_ii[i];
+                const double ziii = (zi * zii * q.omega_prev) /
+                                    (q.omega * q.gamma * (zi - zii) + zi * q.omega_prev * (1.0 - st->shift[i] * q.omega));
+                q.zeta_iii[i] = ziii;
+                q.omegas[i] = q.omega * ziii / zii;
+            }
+        }
+    }
+};
+
+template <int NR>
+struct FinLambda {
+    MSState *st;
+    __device__ void operator()(const double *tot) const
+    {
+        int any = 0;
+        for (int r = 0; r < NR; r++) {
+            MSRhs &q = st->rhs[r];
+            if (!q.running) continue;
+            q.lambda = tot[r];
+            if (!isfinite(q.lambda)) {
+                st->status = 2;
+                q.running_next = 0;
+                continue;
+            }
+            q.gamma = q.lambda / q.delta;
+            int nact = 0;
+            for (int i = 0; i < st->nshift; i++) {
+                if (!q.active[i]) continue;
+                q.gammas[i] = q.gamma * q.zeta_iii[i] * q.omegas[i] / (q.zeta_ii[i] * q.omega);
+                const double fact = sqrt(q.delta * q.zeta_ii[i] * q.zeta_ii[i]);
+                q.active_next[i] = (fact < st->tgt[i]) ? 0 : 1;
+                nact += q.active_next[i];
+                q.zeta_i[i] = q.zeta_ii[i];
+                q.zeta_ii[i] = q.zeta_iii[i];
+            }
+            q.delta = q.lambda;
+            q.iter++;
+            int done = (sqrt(q.lambda) <= st->res) || (st->stop_on_frozen && nact == 0);
+            if (!done && q.iter >= st->max_iter) {
+                done = 1;
+                st->status = (st->status == 0) ? 1 : st->status;
+            }
+            q.running_next = !done;
+            any |= q.running_next;
+        }
+        for (int r = NR; r < st->nrhs; r++) any |= st->rhs[r].running_next;
+        if (!any) st->stop = 1;
+    }
+};
+
+// ------------------------------------------------------------------ vector kernels
+template <typename Rv>
+struct MSVec {
+    typedef typename SpinorT<Rv>::elem E;
+};
+
+// x_i = 0, r = p = p_i = b (b FP64 internal), |b|^2
+template <typename Rv, int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) ms_init_kernel(int Vh, int nshift, size_t stride, const double2 *__restrict__ b,
+                                                             typename MSVec<Rv>::E *r, typename MSVec<Rv>::E *p,
+                                                             typename MSVec<Rv>::E *ps, typename MSVec<Rv>::E *x,
+                                                             double *partials, unsigned *ticket, MSState *st)
+{
+    typedef typename MSVec<Rv>::E E;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[NR];
+#pragma unroll
+    for (int j = 0; j < NR; j++) red[j] = 0.0;
+    if (k < Vh) {
+#pragma unroll
+        for (int j = 0; j < NR; j++) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = j * stride + (size_t)c * Vh + k;
+                const double2 v = b[o];
+                red[j] += v.x * v.x + v.y * v.y;
+                E e;
+                e.x = (Rv)v.x;
+                e.y = (Rv)v.y;
+                r[o] = e;
+                p[o] = e;
+                E z;
+                z.x = 0;
+                z.y = 0;
+                for (int i = 0; i < nshift; i++) {
+                    const size_t oi = (size_t)(j * nshift + i) * stride + (size_t)c * Vh + k;
+                    ps[oi] = e;
+                    x[oi] = z;
+                }
+            }
+        }
+    }
+    FinInit fin{st};
+    reduce_finalize<NR>(red, partials, ticket, fin);
+}
+
+// r += omega s, |r|^2 per RHS
+template <typename Rv, int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) ms_resid_kernel(int Vh, size_t stride, typename MSVec<Rv>::E *r,
+                                                              const typename MSVec<Rv>::E *__restrict__ s, double *partials,
+                                                              unsigned *ticket, MSState *st)
+{
+    typedef typename MSVec<Rv>::E E;
+    if (*(volatile int *)&st->stop) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[NR];
+#pragma unroll
+    for (int j = 0; j < NR; j++) red[j] = 0.0;
+    if (k < Vh) {
+#pragma unroll
+        for (int j = 0; j < NR; j++) {
+            if (!st->rhs[j].running) continue;
+            const Rv om = (Rv)st->rhs[j].omega;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = j * stride + (size_t)c * Vh + k;
+                E rv = r[o];
+                const E sv = s[o];
+                rv.x = rv.x + om * sv.x;
+                rv.y = rv.y + om * sv.y;
+                r[o] = rv;
+                red[j] += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+            }
+        }
+    }
+    FinLambda<NR> fin{st};
+    reduce_finalize<NR>(red, partials, ticket, fin);
+}
+
+// p = r + gamma p ; x_i -= omega_i p_i ; p_i = zeta'''_i r + gamma_i p_i
+template <typename Rv, int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) ms_update_kernel(int Vh, int nshift, size_t stride,
+                                                               const typename MSVec<Rv>::E *__restrict__ r,
+                                                               typename MSVec<Rv>::E *p, typename MSVec<Rv>::E *ps,
+                                                               typename MSVec<Rv>::E *x, MSState *st)
+{
+    typedef typename MSVec<Rv>::E E;
+    __shared__ Rv s_om[NR][MS_MAX_SHIFT], s_ze[NR][MS_MAX_SHIFT], s_ga[NR][MS_MAX_SHIFT];
+    __shared__ int s_act[NR][MS_MAX_SHIFT];
+    __shared__ Rv s_gamma[NR];
+    __shared__ int s_run[NR];
+    if (*(volatile int *)&st->stop_k4) return;
+    for (int t = threadIdx.x; t < NR * MS_MAX_SHIFT; t += blockDim.x) {
+        const int j = t / MS_MAX_SHIFT, i = t % MS_MAX_SHIFT;
+        const MSRhs &q = st->rhs[j];
+        s_act[j][i] = (i < nshift) ? q.active[i] : 0;
+        s_om[j][i] = (Rv)q.omegas[i];
+        s_ze[j][i] = (Rv)q.zeta_iii[i];
+        s_ga[j][i] = (Rv)q.gammas[i];
+        if (i == 0) {
+            s_gamma[j] = (Rv)q.gamma;
+            s_run[j] = q.running;
+        }
+    }
+    __syncthreads();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Vh) return;
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        if (!s_run[j]) continue;
+        E rv[3];
+        const Rv g = s_gamma[j];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const size_t o = j * stride + (size_t)c * Vh + k;
+            rv[c] = r[o];
+            E pv = p[o];
+            pv.x = rv[c].x + g * pv.x;
+            pv.y = rv[c].y + g * pv.y;
+            p[o] = pv;
+        }
+        for (int i = 0; i < nshift; i++) {
+            if (!s_act[j][i]) continue;
+            const Rv om = s_om[j][i], ze = s_ze[j][i], ga = s_ga[j][i];
+            const size_t base = (size_t)(j * nshift + i) * stride + k;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = base + (size_t)c * Vh;
+                E pv = ps[o];
+                E xv = x[o];
+                xv.x = xv.x - om * pv.x;
+                xv.y = xv.y - om * pv.y;
+                pv.x = ze * rv[c].x + ga * pv.x;
+                pv.y = ze * rv[c].y + ga * pv.y;
+                x[o] = xv;
+                ps[o] = pv;
+            }
+        }
+    }
+}
+
+}  // namespace rhmc

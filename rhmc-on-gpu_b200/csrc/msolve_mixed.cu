@@ -1,0 +1,648 @@
+// msolve_mixed.cu -- the mixed-precision batched multi-shift solver and the extern "C"
+// multi-shift entry points.
+//
+// Mixed mode (no counterpart in the reference, which picks FP32 or FP64 per call by the
+// requested residual, lib/Action/Inverter/cu_inverter.cc:45-60):
+//   Phase A  multi-shift CG (msolve.cuh) with FP32 links/vectors, all right-hand sides
+//            batched (every link load serves every RHS), base operator M^dag M + sigma_min,
+//            until every shift reaches tol_A |b| (FP64 scalars and reductions).
+//   Phase B  every (RHS, shift) system is refined by CG in FP32 with FP64 reliable updates
+//            (Sleijpen & van der Vorst): once a system's FP32 residual has dropped by a factor
+//            delta since its last update it waits; every n_ru iterations the waiting systems
+//            add their FP32 correction to the FP64 solution and recompute the residual
+//            b - (M^dag M + sigma) x in FP64 with FP64 links.  A system is finished only when
+//            that FP64 true residual is <= the target.  Systems are sorted by shift and refined
+//            in batches of up to 8 that share link loads.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "capi_util.h"
+#include "context.h"
+#include "kernels.h"
+#include "msolve.cuh"
+#include "solver.h"
+
+namespace rhmc {
+
+constexpr int RB_MAX = 8;
+
+struct ResidCoef {
+    double coef[8];  // mass^2 + sigma of each batched system
+};
+
+struct RBState {
+    int stop;         // every system converged (or failed)
+    int status;       // 0 ok, 2 non-finite
+    int nsys;
+    int first;        // the next reliable update is the initial one (sets p = r)
+    int ru_count;
+    int iters;        // sloppy iterations performed
+    int any_pending;  // some system waits for a reliable update
+    int ru_max;       // force an update after this many sloppy iterations
+    double delta2;    // update when |r_sloppy|^2 <= delta2 |r at last update|^2
+    double tgt[RB_MAX];
+    double rr[RB_MAX];     // |r_sloppy|^2
+    double rr_ru[RB_MAX];  // |r|^2 at the last reliable update
+    double alpha[RB_MAX], beta[RB_MAX];
+    double r2true[RB_MAX];
+    int conv[RB_MAX];
+    int pending[RB_MAX];   // waiting for the next reliable update
+    int hold[RB_MAX];      // skipped by the sloppy iteration
+    int since[RB_MAX];     // sloppy iterations since the last update
+};
+
+// x += xs (FP64 += FP32), xs = 0, for systems not yet converged
+template <int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_accum_kernel(int Vh, size_t stride, double2 *x, float2 *xs, const RBState *st)
+{
+    if (*(volatile const int *)&st->stop || !*(volatile const int *)&st->any_pending) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Vh) return;
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        if (st->conv[j] || !st->pending[j]) continue;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const size_t o = j * stride + (size_t)c * Vh + k;
+            double2 xv = x[o];
+            float2 d = xs[o];
+            xv.x += (double)d.x;
+            xv.y += (double)d.y;
+            x[o] = xv;
+            xs[o] = make_float2(0.f, 0.f);
+        }
+    }
+}
+
+template <int NR>
+struct FinRU {
+    RBState *st;
+    __device__ void operator()(const double *tot) const
+    {
+        int all = 1;
+        for (int j = 0; j < NR; j++) {
+            if (st->conv[j]) continue;
+            if (st->pending[j]) {
+                const double r2 = tot[j];
+                st->pending[j] = 0;
+                st->since[j] = 0;
+                if (!isfinite(r2)) {
+                    st->status = 2;
+                    st->conv[j] = 1;
+                    continue;
+                }
+                st->r2true[j] = r2;
+                st->rr[j] = r2;
+                st->rr_ru[j] = r2;
+                if (sqrt(r2) <= st->tgt[j]) st->conv[j] = 1;
+            }
+            all &= st->conv[j];
+        }
+        st->first = 0;
+        st->ru_count++;
+        st->any_pending = 0;
+        if (all) st->stop = 1;
+    }
+};
+
+// r = b - coef*x - t (FP64), rs = (float) r, |r|^2; on the first update p = rs
+template <int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_resid_kernel(int Vh, size_t stride, const double2 *__restrict__ b,
+                                                              const double2 *__restrict__ x, const double2 *__restrict__ t,
+                                                              float2 *rs, float2 *p, ResidCoef co, double *partials,
+                                                              unsigned *ticket, RBState *st)
+{
+    if (*(volatile const int *)&st->stop || !*(volatile const int *)&st->any_pending) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[NR];
+#pragma unroll
+    for (int j = 0; j < NR; j++) red[j] = 0.0;
+    const int first = st->first;
+    if (k < Vh) {
+#pragma unroll
+        for (int j = 0; j < NR; j++) {
+            if (st->conv[j] || !st->pending[j]) continue;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = j * stride + (size_t)c * Vh + k;
+                const double2 bv = b[o], xv = x[o], tv = t[o];
+                const double re = bv.x - co.coef[j] * xv.x - tv.x, im = bv.y - co.coef[j] * xv.y - tv.y;
+                red[j] += re * re + im * im;
+                const float2 f = make_float2((float)re, (float)im);
+                rs[o] = f;
+                if (first) p[o] = f;
+            }
+        }
+    }
+    FinRU<NR> fin{st};
+    reduce_finalize<NR>(red, partials, ticket, fin);
+}
+
+template <int NR>
+struct FinRBAlpha {
+    RBState *st;
+    __device__ void operator()(const double *tot) const
+    {
+        for (int j = 0; j < NR; j++) {
+            const double pap = tot[2 * j];
+            st->hold[j] = st->pending[j];
+            const int skip = st->conv[j] || st->hold[j];
+            st->alpha[j] = (skip || !(pap > 0.0)) ? 0.0 : st->rr[j] / pap;
+            if (!skip && !isfinite(pap)) st->status = 2;
+        }
+        st->iters++;
+    }
+};
+
+template <int NR>
+struct FinRBBeta {
+    RBState *st;
+    __device__ void operator()(const double *tot) const
+    {
+        for (int j = 0; j < NR; j++) {
+            if (st->conv[j] || st->hold[j]) { st->beta[j] = 0.0; continue; }
+            const double rn = tot[j];
+            st->beta[j] = (st->rr[j] > 0.0) ? rn / st->rr[j] : 0.0;
+            st->rr[j] = rn;
+            st->since[j]++;
+            if (rn <= st->delta2 * st->rr_ru[j] || st->since[j] >= st->ru_max || !isfinite(rn)) {
+                st->pending[j] = 1;
+                st->any_pending = 1;
+            }
+        }
+    }
+};
+
+// xs += alpha p ; rs -= alpha Ap ; |rs|^2
+template <int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride, float2 *xs, float2 *rs,
+                                                           const float2 *__restrict__ p, const float2 *__restrict__ ap,
+                                                           double *partials, unsigned *ticket, RBState *st)
+{
+    if (*(volatile const int *)&st->stop) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[NR];
+#pragma unroll
+    for (int j = 0; j < NR; j++) red[j] = 0.0;
+    if (k < Vh) {
+#pragma unroll
+        for (int j = 0; j < NR; j++) {
+            if (st->conv[j] || st->hold[j]) continue;
+            const float a = (float)st->alpha[j];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = j * stride + (size_t)c * Vh + k;
+                const float2 pv = p[o], av = ap[o];
+                float2 xv = xs[o], rv = rs[o];
+                xv.x += a * pv.x;
+                xv.y += a * pv.y;
+                rv.x -= a * av.x;
+                rv.y -= a * av.y;
+                xs[o] = xv;
+                rs[o] = rv;
+                red[j] += (double)rv.x * rv.x + (double)rv.y * rv.y;
+            }
+        }
+    }
+    FinRBBeta<NR> fin{st};
+    reduce_finalize<NR>(red, partials, ticket, fin);
+}
+
+// p = rs + beta p
+template <int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_p_kernel(int Vh, size_t stride, const float2 *__restrict__ rs, float2 *p,
+                                                          const RBState *st)
+{
+    if (*(volatile const int *)&st->stop) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Vh) return;
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        if (st->conv[j] || st->hold[j]) continue;
+        const float be = (float)st->beta[j];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const size_t o = j * stride + (size_t)c * Vh + k;
+            const float2 rv = rs[o];
+            float2 pv = p[o];
+            pv.x = rv.x + be * pv.x;
+            pv.y = rv.y + be * pv.y;
+            p[o] = pv;
+        }
+    }
+}
+
+template <typename E>
+__global__ void convert_kernel(long n, double2 *dst, const E *src)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        E v = src[i];
+        dst[i] = make_double2((double)v.x, (double)v.y);
+    }
+}
+
+// ------------------------------------------------------------------ Phase B driver
+template <class LF, int NR>
+static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double *tgt, double2 *xg, const double2 *bg,
+                    int max_iter, int n_ru, long *iters_out, int *ru_out)
+{
+    AuxScope aux_scope(c);
+    cudaStream_t s_ = c->aux;
+    const int Vh = (int)c->Vh;
+    const size_t stride = 3 * (size_t)Vh;
+    void *xs, *rs, *p, *ap, *h, *h64, *t64, *stv, *part, *tick;
+    const size_t v32 = stride * sizeof(float2), v64 = stride * sizeof(double2);
+    CK(c->ws.get("rb_xs", NR * v32, &xs));
+    CK(c->ws.get("rb_rs", NR * v32, &rs));
+    CK(c->ws.get("rb_p", NR * v32, &p));
+    CK(c->ws.get("rb_ap", NR * v32, &ap));
+    CK(c->ws.get("rb_h", NR * v32, &h));
+    CK(c->ws.get("rb_h64", NR * v64, &h64));
+    CK(c->ws.get("rb_t64", NR * v64, &t64));
+    CK(c->ws.get("rb_state", sizeof(RBState), &stv));
+    const int gd = dslash_grid(c), gv = grid_for(Vh, VEC_BLOCK);
+    CK(c->ws.get("rb_partials", (size_t)(gd > gv ? gd : gv) * 2 * NR * sizeof(double), &part));
+    CK(c->ws.get("rb_tickets", 4 * sizeof(unsigned), &tick));
+    L64_18 l64;
+    links_f64_18(c, &l64);
+    RBState *st = (RBState *)stv;
+    unsigned *tk = (unsigned *)tick;
+    double *pt = (double *)part;
+
+    RBState h0;
+    memset(&h0, 0, sizeof(h0));
+    h0.nsys = NR;
+    h0.first = 1;
+    h0.any_pending = 1;
+    h0.delta2 = 0.05 * 0.05;
+    h0.ru_max = 2000;
+    for (int j = 0; j < NR; j++) {
+        h0.tgt[j] = tgt[j];
+        h0.pending[j] = 1;
+    }
+    CK(cudaMemcpyAsync(st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemsetAsync(tk, 0, 4 * sizeof(unsigned), s_));
+    CK(cudaMemsetAsync(xs, 0, NR * v32, s_));
+
+    ResidCoef co;
+    for (int j = 0; j < 8; j++) co.coef[j] = coef[j < NR ? j : 0];
+
+    // FP64 M^dag M pieces of the reliable update
+    DslashArgs<L64_18, NR, NoFin> d1;
+    memset(&d1, 0, sizeof(d1));
+    d1.g = c->g; d1.p_out = 1; d1.links = l64; d1.in = xg; d1.out = (double2 *)h64; d1.stride = stride; d1.beta = 0.5;
+    d1.stop = &st->stop;
+    d1.run_if = &st->any_pending;
+    DslashArgs<L64_18, NR, NoFin> d2 = d1;
+    d2.p_out = 0; d2.in = (const double2 *)h64; d2.out = (double2 *)t64; d2.beta = -0.5;
+    // FP32 sloppy operator
+    typedef typename LF::real Rs;
+    DslashArgs<LF, NR, NoFin> s1;
+    memset(&s1, 0, sizeof(s1));
+    s1.g = c->g; s1.p_out = 1; s1.links = lf; s1.in = (const float2 *)p; s1.out = (float2 *)h; s1.stride = stride;
+    s1.beta = (Rs)0.5; s1.stop = &st->stop;
+    DslashArgs<LF, NR, FinRBAlpha<NR>> s2;
+    memset(&s2, 0, sizeof(s2));
+    s2.g = c->g; s2.p_out = 0; s2.links = lf; s2.in = (const float2 *)h; s2.out = (float2 *)ap; s2.y = (const float2 *)p;
+    s2.stride = stride; s2.beta = (Rs)-0.5; s2.use_alphas = 1;
+    for (int j = 0; j < NR; j++) s2.alphas[j] = (Rs)coef[j];
+    s2.partials = pt; s2.ticket = tk + 1; s2.fin.st = st; s2.stop = &st->stop;
+
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+    rb_accum_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (float2 *)xs, st);
+    dslash_kernel<L64_18, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(d1);
+    dslash_kernel<L64_18, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(d2);
+    rb_resid_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, bg, xg, (const double2 *)t64, (float2 *)rs, (float2 *)p, co,
+                                                         pt, tk, st);
+    for (int it = 0; it < n_ru; it++) {
+        dslash_kernel<LF, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(s1);
+        dslash_kernel<LF, NR, true, true, FinRBAlpha<NR>><<<gd, DSLASH_BLOCK, 0, s_>>>(s2);
+        rb_xr_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (float2 *)xs, (float2 *)rs, (const float2 *)p,
+                                                          (const float2 *)ap, pt, tk + 2, st);
+        rb_p_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const float2 *)rs, (float2 *)p, st);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s_, &graph);
+    if (ce != cudaSuccess) return cuda_fail(ce, "refine capture");
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_fail(ce, "refine instantiate");
+
+    int *hflag = c->hflags;
+    cudaEvent_t ev[2];
+    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    const long max_rep = max_iter / n_ru + 2;
+    long rep = 0;
+    bool done = false;
+    hflag[0] = hflag[1] = 0;
+    const bool dbg = getenv("RHMC_DEBUG") != nullptr;
+    for (; rep < max_rep && !done; rep++) {
+        ce = cudaGraphLaunch(exec, s_);
+        if (ce != cudaSuccess) break;
+        if (dbg) {
+            RBState d;
+            cudaMemcpyAsync(&d, st, sizeof(d), cudaMemcpyDeviceToHost, s_);
+            cudaStreamSynchronize(s_);
+            fprintf(stderr, "[refine n=%d rep=%ld iters=%d ru=%d stop=%d status=%d]", NR, rep, d.iters, d.ru_count, d.stop, d.status);
+            for (int j = 0; j < NR; j++)
+                fprintf(stderr, " (%d%d r2t=%.3e rr=%.3e)", d.conv[j], d.pending[j], d.r2true[j], d.rr[j]);
+            fprintf(stderr, "\n");
+        }
+        cudaMemcpyAsync(&hflag[rep & 1], &st->stop, sizeof(int), cudaMemcpyDeviceToHost, s_);
+        cudaEventRecord(ev[rep & 1], s_);
+        if (rep >= 1) {
+            cudaEventSynchronize(ev[(rep - 1) & 1]);
+            if (hflag[(rep - 1) & 1]) done = true;
+        }
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s_);
+    c->launches += rep * (4 + 4 * (long)n_ru);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    cudaGraphExecDestroy(exec);
+    if (ce != cudaSuccess) return cuda_fail(ce, "refine loop");
+    RBState hs;
+    CK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
+    *iters_out += hs.iters;
+    *ru_out += hs.ru_count;
+    if (hs.status == 2) return fail(RHMC_ERR_NONFINITE, "refinement: non-finite reduction");
+    if (!hs.stop) return fail(RHMC_ERR_MAXITER, "refinement: iteration cap %d reached", max_iter);
+    return RHMC_OK;
+}
+
+template <class LF>
+static int rb_group_n(rhmc_ctx *c, const LF &lf, int n, const double *coef, const double *tgt, double2 *xg, const double2 *bg,
+                      int max_iter, int n_ru, long *iters, int *ru)
+{
+    switch (n) {
+    case 1: return rb_group<LF, 1>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
+    case 2: return rb_group<LF, 2>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
+    case 3: return rb_group<LF, 3>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
+    case 4: return rb_group<LF, 4>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
+    case 8: return rb_group<LF, 8>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
+    default: return fail(RHMC_ERR_ARG, "bad refinement batch %d", n);
+    }
+}
+
+// Refine all (rhs, shift) systems of x (FP64 internal [nrhs][nshift]) to |b - A_sigma x| <= res.
+template <class LF>
+static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shifts, int nrhs, double res, int max_iter,
+                      double2 *x, const double2 *b, long *iters, int *ru)
+{
+    const size_t stride = 3 * (size_t)c->Vh;
+    const size_t v64 = stride * sizeof(double2);
+    void *xg, *bg;
+    CK(c->ws.get("rb_xg", RB_MAX * v64, &xg));
+    CK(c->ws.get("rb_bg", RB_MAX * v64, &bg));
+    std::vector<int> order(nshift * nrhs);
+    for (int q = 0; q < nshift * nrhs; q++) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int bq) { return shifts[a % nshift] < shifts[bq % nshift]; });
+    const double m2 = c->mass * c->mass;
+    size_t g0 = 0;
+    while (g0 < order.size()) {
+        const size_t left = order.size() - g0;
+        const int n = left >= 8 ? 8 : (left >= 4 ? 4 : (int)left);  // instantiated batch widths
+        double coef[RB_MAX], tgt[RB_MAX];
+        for (int j = 0; j < n; j++) {
+            const int q = order[g0 + j];
+            coef[j] = m2 + shifts[q % nshift];
+            tgt[j] = res;
+            CK(cudaMemcpyAsync((double2 *)xg + j * stride, x + (size_t)q * stride, v64, cudaMemcpyDeviceToDevice, c->stream));
+            CK(cudaMemcpyAsync((double2 *)bg + j * stride, b + (size_t)(q / nshift) * stride, v64, cudaMemcpyDeviceToDevice,
+                               c->stream));
+        }
+        // iterations between reliable-update stages (systems that need none skip the stage)
+        const double kappa = (16.0 + coef[0]) / coef[0];
+        const int n_ru = kappa > 1e3 ? 16 : 8;
+        int rc = rb_group_n(c, lf, n, coef, tgt, (double2 *)xg, (const double2 *)bg, max_iter, n_ru, iters, ru);
+        if (rc) return rc;
+        for (int j = 0; j < n; j++) {
+            const int q = order[g0 + j];
+            CK(cudaMemcpyAsync(x + (size_t)q * stride, (double2 *)xg + j * stride, v64, cudaMemcpyDeviceToDevice, c->stream));
+        }
+        g0 += n;
+    }
+    return RHMC_OK;
+}
+
+int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrhs, double res, int max_iter, double tolA,
+                 double2 *x, const double2 *b, rhmc_msolve_info *info)
+{
+    if (fmt != RHMC_LINKS_F32_18 && fmt != RHMC_LINKS_F32_12) return fail(RHMC_ERR_ARG, "mixed mode needs an FP32 link format");
+    const size_t stride = 3 * (size_t)c->Vh;
+    auto t0 = std::chrono::steady_clock::now();
+    // |b_r|^2
+    std::vector<double> b2(nrhs);
+    {
+        void *z;
+        CK(c->ws.get("mx_zero", stride * sizeof(double2), &z));
+        CK(cudaMemsetAsync(z, 0, stride * sizeof(double2), c->stream));
+        const double s0 = 0.0;
+        for (int r = 0; r < nrhs; r++) {
+            int rc = true_residuals(c, 1, &s0, 1, (const double2 *)z, b + r * stride, &b2[r]);
+            if (rc) return rc;
+        }
+    }
+    double bmax = 0;
+    for (double v : b2) bmax = std::max(bmax, std::sqrt(v));
+    double smin = shifts[0];
+    for (int i = 1; i < nshift; i++) smin = std::min(smin, shifts[i]);
+    std::vector<double> tgt(nshift, std::max(res, tolA * bmax));
+    void *xa;
+    CK(c->ws.get("mx_xa", (size_t)nrhs * nshift * stride * sizeof(float2), &xa));
+    MSolveArgs A;
+    A.nshift = nshift;
+    A.nrhs = nrhs;
+    A.shift = shifts;
+    A.base_shift = smin;
+    A.tgt = tgt.data();
+    A.res_base = std::max(res, tolA * bmax);
+    A.max_iter = max_iter;
+    A.stop_on_frozen = 1;
+    A.chunk = 8;
+    A.b = b;
+    A.x = xa;
+    MSolveInfo mi;
+    memset(&mi, 0, sizeof(mi));
+    int rc = msolve_shifted(c, fmt, A, &mi);
+    if (rc && rc != RHMC_ERR_MAXITER) return rc;
+    const long n = (long)nrhs * nshift * stride;
+    convert_kernel<float2><<<grid_for(n, 256), 256, 0, c->stream>>>(n, x, (const float2 *)xa);
+    c->launches++;
+    CK(cudaGetLastError());
+    long it_b = 0;
+    int ru = 0;
+    if (fmt == RHMC_LINKS_F32_12) {
+        L32_12 lf;
+        links_f32_12(c, &lf);
+        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru);
+    } else {
+        L32_18 lf;
+        links_f32_18(c, &lf);
+        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    if (info) {
+        info->status = rc;
+        for (int r = 0; r < nrhs && r < 8; r++) info->iters[r] = mi.iters[r];
+        info->refine_iters = it_b;
+        info->reliable_updates = ru;
+        info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return rc;
+}
+
+}  // namespace rhmc
+
+using namespace rhmc;
+
+static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, const double2 *b, rhmc_msolve_info *info)
+{
+    const size_t stride = 3 * (size_t)c->Vh;
+    std::vector<double> tgt(P->nshift, P->residual);
+    int done = 0, rc = RHMC_OK;
+    auto t0 = std::chrono::steady_clock::now();
+    while (done < P->nrhs) {
+        const int left = P->nrhs - done;
+        const int n = left >= 8 ? 8 : (left >= 4 ? 4 : left);
+        MSolveArgs A;
+        A.nshift = P->nshift;
+        A.nrhs = n;
+        A.shift = P->shifts;
+        A.base_shift = 0.0;
+        A.tgt = tgt.data();
+        A.res_base = P->residual;
+        A.max_iter = P->max_iter;
+        A.stop_on_frozen = 1;
+        A.chunk = 8;
+        A.b = b + (size_t)done * stride;
+        A.x = x + (size_t)done * P->nshift * stride;
+        MSolveInfo mi;
+        memset(&mi, 0, sizeof(mi));
+        rc = msolve_shifted(c, P->fmt, A, &mi);
+        if (info)
+            for (int j = 0; j < n && done + j < 8; j++) info->iters[done + j] = mi.iters[j];
+        if (rc) break;
+        done += n;
+    }
+    if (info) {
+        info->status = rc;
+        info->refine_iters = 0;
+        info->reliable_updates = 0;
+        info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return rc;
+}
+
+// The reference's single-precision path (cuda_shifted_inverter, lib/Cuda/cuda_inverter.cu:647-857):
+// the same recurrences with FP32 links and vectors, FP64 scalars; solutions returned in FP64.
+static int msolve_fp32(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, const double2 *b, rhmc_msolve_info *info)
+{
+    const size_t stride = 3 * (size_t)c->Vh;
+    std::vector<double> tgt(P->nshift, P->residual);
+    auto t0 = std::chrono::steady_clock::now();
+    int done = 0, rc = RHMC_OK;
+    void *xa;
+    CK(c->ws.get("mx_xa", (size_t)8 * P->nshift * stride * sizeof(float2), &xa));
+    while (done < P->nrhs) {
+        const int left = P->nrhs - done;
+        const int n = left >= 8 ? 8 : (left >= 4 ? 4 : left);
+        MSolveArgs A;
+        A.nshift = P->nshift;
+        A.nrhs = n;
+        A.shift = P->shifts;
+        A.base_shift = 0.0;
+        A.tgt = tgt.data();
+        A.res_base = P->residual;
+        A.max_iter = P->max_iter;
+        A.stop_on_frozen = 1;
+        A.chunk = 8;
+        A.b = b + (size_t)done * stride;
+        A.x = xa;
+        MSolveInfo mi;
+        memset(&mi, 0, sizeof(mi));
+        rc = msolve_shifted(c, P->fmt, A, &mi);
+        if (info)
+            for (int j = 0; j < n && done + j < 8; j++) info->iters[done + j] = mi.iters[j];
+        if (rc) break;
+        const long nel = (long)n * P->nshift * stride;
+        convert_kernel<float2><<<grid_for(nel, 256), 256, 0, c->stream>>>(nel, x + (size_t)done * P->nshift * stride, (const float2 *)xa);
+        c->launches++;
+        CK(cudaGetLastError());
+        done += n;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    if (info) {
+        info->status = rc;
+        info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return rc;
+}
+
+extern "C" {
+
+int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const double *b, rhmc_msolve_info *info)
+{
+    if (!c || !P || !x || !b || !P->shifts) return fail(RHMC_ERR_ARG, "null argument");
+    if (P->nshift < 1 || P->nshift > MS_MAX_SHIFT) return fail(RHMC_ERR_ARG, "nshift must be in [1, %d]", MS_MAX_SHIFT);
+    if (P->nrhs < 1) return fail(RHMC_ERR_ARG, "nrhs must be >= 1");
+    if (P->max_iter < 1) return fail(RHMC_ERR_ARG, "max_iter must be >= 1");
+    for (int i = 0; i < P->nshift; i++)
+        if (!(P->shifts[i] >= 0.0)) return fail(RHMC_ERR_ARG, "shifts must be >= 0");
+    if (info) memset(info, 0, sizeof(*info));
+    if (P->mode == RHMC_MSOLVE_FP64) {
+        if (P->fmt != RHMC_LINKS_F64_18 && P->fmt != RHMC_LINKS_F64_12) return fail(RHMC_ERR_ARG, "FP64 mode needs FP64 links");
+        return msolve_fp64(c, P, (double2 *)x, (const double2 *)b, info);
+    }
+    if (P->mode == RHMC_MSOLVE_FP32) {
+        if (P->fmt != RHMC_LINKS_F32_18 && P->fmt != RHMC_LINKS_F32_12) return fail(RHMC_ERR_ARG, "FP32 mode needs FP32 links");
+        return msolve_fp32(c, P, (double2 *)x, (const double2 *)b, info);
+    }
+    if (P->mode == RHMC_MSOLVE_MIXED) {
+        if (P->nrhs > MS_MAX_RHS) return fail(RHMC_ERR_ARG, "mixed mode batches at most %d right-hand sides", MS_MAX_RHS);
+        const int nr = P->nrhs;
+        if (!(nr == 1 || nr == 2 || nr == 3 || nr == 4 || nr == 8)) return fail(RHMC_ERR_ARG, "mixed mode nrhs must be 1,2,3,4 or 8");
+        const double tolA = P->tol_phase_a > 0 ? P->tol_phase_a : 3e-6;
+        return msolve_mixed(c, P->fmt, P->nshift, P->shifts, nr, P->residual, P->max_iter, tolA, (double2 *)x, (const double2 *)b,
+                            info);
+    }
+    return fail(RHMC_ERR_ARG, "bad solver mode %d", P->mode);
+}
+
+int rhmc_msolve_host(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const double *b, rhmc_msolve_info *info)
+{
+    if (!c || !P || !x || !b) return fail(RHMC_ERR_ARG, "null argument");
+    const size_t stride = 3 * (size_t)c->Vh;
+    const size_t nb = (size_t)P->nrhs, nx = (size_t)P->nrhs * P->nshift;
+    void *bi, *xi, *tmp;
+    CK(c->ws.get("mh_b", nb * stride * sizeof(double2), &bi));
+    CK(c->ws.get("mh_x", nx * stride * sizeof(double2), &xi));
+    CK(c->ws.get("mh_tmp", (nx > nb ? nx : nb) * stride * sizeof(double2), &tmp));
+    CK(cudaMemcpyAsync(tmp, b, nb * stride * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    launch_spinor_to_internal(c, true, bi, (const double *)tmp, (int)nb);
+    int rc = rhmc_msolve(c, P, (double *)xi, (const double *)bi, info);
+    if (rc) return rc;
+    launch_spinor_from_internal(c, true, (double *)tmp, xi, (int)nx);
+    CK(cudaMemcpyAsync(x, tmp, nx * stride * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return RHMC_OK;
+}
+
+int rhmc_true_residuals(rhmc_ctx *c, int nshift, const double *shifts, int nrhs, const double *x, const double *b, double *out)
+{
+    if (!c || !shifts || !x || !b || !out || nshift < 1 || nrhs < 1) return fail(RHMC_ERR_ARG, "bad argument");
+    int rc = true_residuals(c, nshift, shifts, nrhs, (const double2 *)x, (const double2 *)b, out);
+    if (rc) return rc;
+    for (int i = 0; i < nshift * nrhs; i++) out[i] = std::sqrt(out[i]);
+    return RHMC_OK;
+}
+
+}  // extern "C"

@@ -289,4 +289,41 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double *smem)
     __syncthreads();
 }
 
+// Grid-wide deterministic reduction: every block writes its N block sums to
+// partials[block][N]; the last block to finish (atomic ticket) re-reads all partials in
+// block order, sums them and hands the totals to fin() in thread 0, then re-arms the ticket.
+// All threads of every block must call it.
+struct NoFin {
+    __device__ void operator()(const double *) const {}
+};
+
+template <int N, class FIN>
+__device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials, unsigned *ticket, const FIN &fin)
+{
+    __shared__ double smem[N * 32];
+    __shared__ int am_last;
+    block_sum<N>(v, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < N; j++) partials[(size_t)blockIdx.x * N + j] = v[j];
+        __threadfence();
+        unsigned t = atomicAdd(ticket, 1u);
+        am_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    double acc[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) acc[j] = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+#pragma unroll
+        for (int j = 0; j < N; j++) acc[j] += __ldcg(partials + (size_t)i * N + j);
+    block_sum<N>(acc, smem);
+    if (threadIdx.x == 0) {
+        *ticket = 0;
+        fin(acc);
+    }
+}
+
 }  // namespace rhmc

@@ -174,3 +174,62 @@ class Context:
 
     def mdagm(self, fmt, out, inp, shift=0.0, n=1):
         self.call("rhmc_mdagm", fmt, out, inp, float(shift), n)
+
+
+MSOLVE_FP64, MSOLVE_MIXED, MSOLVE_FP32 = 0, 1, 2
+
+
+class MsolveParams(ctypes.Structure):
+    _fields_ = [("nshift", ctypes.c_int), ("shifts", ctypes.POINTER(ctypes.c_double)), ("nrhs", ctypes.c_int),
+                ("residual", ctypes.c_double), ("max_iter", ctypes.c_int), ("mode", ctypes.c_int), ("fmt", ctypes.c_int),
+                ("tol_phase_a", ctypes.c_double)]
+
+
+class MsolveInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iters", ctypes.c_int * 8), ("refine_iters", ctypes.c_long),
+                ("reliable_updates", ctypes.c_int), ("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"status": self.status, "iters": list(self.iters), "refine_iters": self.refine_iters,
+                "reliable_updates": self.reliable_updates, "seconds": self.seconds}
+
+
+def _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a=0.0):
+    sh = np.ascontiguousarray(shifts, np.float64)
+    p = MsolveParams(len(sh), sh.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nrhs, residual, max_iter, mode, fmt,
+                     tol_phase_a)
+    p._keep = sh
+    return p
+
+
+def _ctx_msolve(self, x, b, shifts, residual, nrhs=1, max_iter=100000, mode=MSOLVE_FP64, fmt=LINKS_F64_18, tol_phase_a=0.0):
+    """x, b: device FP64 internal spinors (b: nrhs, x: nrhs*nshift, RHS-major)."""
+    p = _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a)
+    info = MsolveInfo()
+    self.call("rhmc_msolve", ctypes.byref(p), x, b, ctypes.byref(info))
+    return info.as_dict()
+
+
+def _ctx_msolve_host(self, b, shifts, residual, max_iter=100000, mode=MSOLVE_FP64, fmt=LINKS_F64_18, tol_phase_a=0.0):
+    """b: numpy complex (Vh,3) or (nrhs,Vh,3) reference layout.  Returns (x, info) with x of shape
+    (nshift,Vh,3) or (nrhs,nshift,Vh,3)."""
+    b = np.ascontiguousarray(b, np.complex128)
+    single = b.ndim == 2
+    nrhs = 1 if single else b.shape[0]
+    x = np.zeros((nrhs, len(shifts), self.Vh, 3), np.complex128)
+    p = _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a)
+    info = MsolveInfo()
+    self.call("rhmc_msolve_host", ctypes.byref(p), x, b, ctypes.byref(info))
+    return (x[0] if single else x), info.as_dict()
+
+
+def _ctx_true_residuals(self, x, b, shifts, nrhs=1):
+    sh = np.ascontiguousarray(shifts, np.float64)
+    out = np.zeros((nrhs, len(sh)), np.float64)
+    self.call("rhmc_true_residuals", len(sh), sh, nrhs, x, b, out)
+    return out
+
+
+Context.msolve = _ctx_msolve
+Context.msolve_host = _ctx_msolve_host
+Context.true_residuals = _ctx_true_residuals
