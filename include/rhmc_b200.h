@@ -100,6 +100,9 @@ int rhmc_spinor_from_internal(rhmc_ctx *ctx, int fmt, double *ref, const void *i
  * including the factor 1/2), for n right-hand sides sharing each link load.  in/out are
  * internal-layout device spinors of the precision of `fmt`. */
 int rhmc_dslash(rhmc_ctx *ctx, int fmt, int parity_out, void *out, const void *in, int n);
+/* `repeats` times: odd = D_oe even, then even = D_eo odd (n RHS), issued back to back from C
+ * so that timing loops measure the kernels and not the caller's launch overhead. */
+int rhmc_dslash_repeat(rhmc_ctx *ctx, int fmt, void *even, void *odd, int n, int repeats);
 /* Reference-facing form of Deo/Doe: host spinors in the reference layout, FP64 links.
  * Copies in, applies, copies out (used for the end-to-end measurement). */
 int rhmc_dslash_host(rhmc_ctx *ctx, int parity_out, double *out, const double *in);
@@ -112,9 +115,11 @@ enum {
     RHMC_MSOLVE_FP64 = 0,  /* the reference algorithm in FP64 (multips_shifted_invert,
                               lib/Action/Inverter/inverter.cc:142-339): base operator M^dag M,
                               shift frozen when sqrt(|r|^2 zeta^2) < residual */
-    RHMC_MSOLVE_MIXED = 1, /* FP32 multi-shift on the smallest pole, all RHS batched, then FP32
-                              CG per system with FP64 reliable updates until every FP64 true
-                              residual |b - (M^dag M + sigma_i) x_i| <= residual */
+    RHMC_MSOLVE_MIXED = 1, /* multi-shift on the smallest pole with all RHS batched (FP32 links and
+                              vectors to tol_phase_a |b| with an FP32 fmt; FP64 vectors to
+                              `residual` with an FP64 fmt, 12-real links when fmt says so), then
+                              FP32 CG per system inside FP64 defect correction until every FP64
+                              true residual |b - (M^dag M + sigma_i) x_i| <= residual */
     RHMC_MSOLVE_FP32 = 2   /* the reference algorithm with FP32 links and vectors (its
                               single-precision path, lib/Cuda/cuda_inverter.cu:647-857, used
                               when residual >= 1e-4, cu_inverter.cc:45-60); FP64 scalars */
@@ -127,8 +132,13 @@ typedef struct {
     double residual;       /* absolute stopping residual (residue_metro / residue_md, parameters.h:68,73) */
     int max_iter;          /* iteration cap (max_cg, parameters.h:57) */
     int mode;              /* RHMC_MSOLVE_* */
-    int fmt;               /* link format: FP64 ones for RHMC_MSOLVE_FP64, FP32 ones for RHMC_MSOLVE_MIXED */
+    int fmt;               /* link format of the multi-shift phase (FP64 ones for RHMC_MSOLVE_FP64,
+                              FP32 ones for RHMC_MSOLVE_FP32, any for RHMC_MSOLVE_MIXED) */
     double tol_phase_a;    /* mixed mode: relative residual of the FP32 multi-shift phase (0: 3e-6) */
+    double ru_delta;       /* mixed mode: FP32 residual reduction between FP64 updates (0: 0.05) */
+    int certify;           /* FP64 mode: afterwards refine, by FP64 CG one system at a time, every system
+                              whose FP64 true residual is still above `residual` (the reference's
+                              iterated-residual test alone can stop above it) */
 } rhmc_msolve_params;
 
 typedef struct {

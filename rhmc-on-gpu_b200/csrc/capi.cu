@@ -246,6 +246,18 @@ int rhmc_dslash(rhmc_ctx *c, int fmt, int parity_out, void *out, const void *in,
     return RHMC_OK;
 }
 
+int rhmc_dslash_repeat(rhmc_ctx *c, int fmt, void *even, void *odd, int n, int repeats)
+{
+    if (!c || !even || !odd || n <= 0 || repeats < 0 || fmt < 0 || fmt > 3) return fail(RHMC_ERR_ARG, "bad argument");
+    const size_t stride = 3 * (size_t)c->Vh;
+    for (int r = 0; r < repeats; r++) {
+        cudaError_t e = launch_dslash(c, fmt, 1, odd, even, stride, n, nullptr, 0.0, 0.5, nullptr, nullptr);
+        if (e == cudaSuccess) e = launch_dslash(c, fmt, 0, even, odd, stride, n, nullptr, 0.0, 0.5, nullptr, nullptr);
+        if (e != cudaSuccess) return cuda_fail(e, "rhmc_dslash_repeat");
+    }
+    return RHMC_OK;
+}
+
 int rhmc_dslash_host(rhmc_ctx *c, int parity_out, double *out, const double *in)
 {
     if (!c || !out || !in || (parity_out != 0 && parity_out != 1)) return fail(RHMC_ERR_ARG, "bad argument");

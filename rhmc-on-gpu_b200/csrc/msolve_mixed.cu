@@ -6,13 +6,14 @@
 //   Phase A  multi-shift CG (msolve.cuh) with FP32 links/vectors, all right-hand sides
 //            batched (every link load serves every RHS), base operator M^dag M + sigma_min,
 //            until every shift reaches tol_A |b| (FP64 scalars and reductions).
-//   Phase B  every (RHS, shift) system is refined by CG in FP32 with FP64 reliable updates
-//            (Sleijpen & van der Vorst): once a system's FP32 residual has dropped by a factor
-//            delta since its last update it waits; every n_ru iterations the waiting systems
-//            add their FP32 correction to the FP64 solution and recompute the residual
-//            b - (M^dag M + sigma) x in FP64 with FP64 links.  A system is finished only when
-//            that FP64 true residual is <= the target.  Systems are sorted by shift and refined
-//            in batches of up to 8 that share link loads.
+//   Phase B  every (RHS, shift) system is refined by FP32 CG inside an FP64 defect correction:
+//            once a system's FP32 residual has dropped by a factor delta since its last
+//            update it waits; every n_ru iterations the waiting systems add their FP32
+//            correction to the FP64 solution, recompute the residual b - (M^dag M + sigma) x
+//            in FP64 with FP64 links and restart their FP32 CG from it (keeping the old search
+//            direction across the update diverged for kappa ~ 1e5).  A system is finished only
+//            when that FP64 true residual is <= the target.  Systems are sorted by shift and
+//            refined in batches of up to 8 that share link loads.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -57,8 +58,8 @@ struct RBState {
 };
 
 // x += xs (FP64 += FP32), xs = 0, for systems not yet converged
-template <int NR>
-__global__ void __launch_bounds__(VEC_BLOCK) rb_accum_kernel(int Vh, size_t stride, double2 *x, float2 *xs, const RBState *st)
+template <int NR, typename E>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_accum_kernel(int Vh, size_t stride, double2 *x, E *xs, const RBState *st)
 {
     if (*(volatile const int *)&st->stop || !*(volatile const int *)&st->any_pending) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -70,11 +71,13 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_accum_kernel(int Vh, size_t stri
         for (int c = 0; c < 3; c++) {
             const size_t o = j * stride + (size_t)c * Vh + k;
             double2 xv = x[o];
-            float2 d = xs[o];
+            E d = xs[o];
             xv.x += (double)d.x;
             xv.y += (double)d.y;
             x[o] = xv;
-            xs[o] = make_float2(0.f, 0.f);
+            d.x = 0;
+            d.y = 0;
+            xs[o] = d;
         }
     }
 }
@@ -111,10 +114,10 @@ struct FinRU {
 };
 
 // r = b - coef*x - t (FP64), rs = (float) r, |r|^2; on the first update p = rs
-template <int NR>
+template <int NR, typename E>
 __global__ void __launch_bounds__(VEC_BLOCK) rb_resid_kernel(int Vh, size_t stride, const double2 *__restrict__ b,
                                                               const double2 *__restrict__ x, const double2 *__restrict__ t,
-                                                              float2 *rs, float2 *p, ResidCoef co, double *partials,
+                                                              E *rs, E *p, ResidCoef co, double *partials,
                                                               unsigned *ticket, RBState *st)
 {
     if (*(volatile const int *)&st->stop || !*(volatile const int *)&st->any_pending) return;
@@ -122,7 +125,6 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_resid_kernel(int Vh, size_t stri
     double red[NR];
 #pragma unroll
     for (int j = 0; j < NR; j++) red[j] = 0.0;
-    const int first = st->first;
     if (k < Vh) {
 #pragma unroll
         for (int j = 0; j < NR; j++) {
@@ -133,9 +135,11 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_resid_kernel(int Vh, size_t stri
                 const double2 bv = b[o], xv = x[o], tv = t[o];
                 const double re = bv.x - co.coef[j] * xv.x - tv.x, im = bv.y - co.coef[j] * xv.y - tv.y;
                 red[j] += re * re + im * im;
-                const float2 f = make_float2((float)re, (float)im);
+                E f;
+                f.x = re;
+                f.y = im;
                 rs[o] = f;
-                if (first) p[o] = f;
+                p[o] = f;  // restart the search direction from the true residual
             }
         }
     }
@@ -170,7 +174,9 @@ struct FinRBBeta {
             st->beta[j] = (st->rr[j] > 0.0) ? rn / st->rr[j] : 0.0;
             st->rr[j] = rn;
             st->since[j]++;
-            if (rn <= st->delta2 * st->rr_ru[j] || st->since[j] >= st->ru_max || !isfinite(rn)) {
+            // update after a drop by delta, after ru_max iterations, or when the FP32 iteration
+            // stops making progress (its residual above 4x the last true one)
+            if (rn <= st->delta2 * st->rr_ru[j] || st->since[j] >= st->ru_max || !isfinite(rn) || rn > 4.0 * st->rr_ru[j]) {
                 st->pending[j] = 1;
                 st->any_pending = 1;
             }
@@ -179,9 +185,9 @@ struct FinRBBeta {
 };
 
 // xs += alpha p ; rs -= alpha Ap ; |rs|^2
-template <int NR>
-__global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride, float2 *xs, float2 *rs,
-                                                           const float2 *__restrict__ p, const float2 *__restrict__ ap,
+template <int NR, typename E>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride, E *xs, E *rs,
+                                                           const E *__restrict__ p, const E *__restrict__ ap,
                                                            double *partials, unsigned *ticket, RBState *st)
 {
     if (*(volatile const int *)&st->stop) return;
@@ -193,12 +199,13 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride,
 #pragma unroll
         for (int j = 0; j < NR; j++) {
             if (st->conv[j] || st->hold[j]) continue;
-            const float a = (float)st->alpha[j];
+            typedef decltype(E().x) Rs;
+            const Rs a = (Rs)st->alpha[j];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const size_t o = j * stride + (size_t)c * Vh + k;
-                const float2 pv = p[o], av = ap[o];
-                float2 xv = xs[o], rv = rs[o];
+                const E pv = p[o], av = ap[o];
+                E xv = xs[o], rv = rs[o];
                 xv.x += a * pv.x;
                 xv.y += a * pv.y;
                 rv.x -= a * av.x;
@@ -214,8 +221,8 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride,
 }
 
 // p = rs + beta p
-template <int NR>
-__global__ void __launch_bounds__(VEC_BLOCK) rb_p_kernel(int Vh, size_t stride, const float2 *__restrict__ rs, float2 *p,
+template <int NR, typename E>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_p_kernel(int Vh, size_t stride, const E *__restrict__ rs, E *p,
                                                           const RBState *st)
 {
     if (*(volatile const int *)&st->stop) return;
@@ -224,12 +231,13 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_p_kernel(int Vh, size_t stride, 
 #pragma unroll
     for (int j = 0; j < NR; j++) {
         if (st->conv[j] || st->hold[j]) continue;
-        const float be = (float)st->beta[j];
+        typedef decltype(E().x) Rs;
+        const Rs be = (Rs)st->beta[j];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const size_t o = j * stride + (size_t)c * Vh + k;
-            const float2 rv = rs[o];
-            float2 pv = p[o];
+            const E rv = rs[o];
+            E pv = p[o];
             pv.x = rv.x + be * pv.x;
             pv.y = rv.y + be * pv.y;
             p[o] = pv;
@@ -250,14 +258,16 @@ __global__ void convert_kernel(long n, double2 *dst, const E *src)
 // ------------------------------------------------------------------ Phase B driver
 template <class LF, int NR>
 static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double *tgt, double2 *xg, const double2 *bg,
-                    int max_iter, int n_ru, long *iters_out, int *ru_out)
+                    int max_iter, int n_ru, long *iters_out, int *ru_out, double ru_delta)
 {
     AuxScope aux_scope(c);
     cudaStream_t s_ = c->aux;
     const int Vh = (int)c->Vh;
     const size_t stride = 3 * (size_t)Vh;
     void *xs, *rs, *p, *ap, *h, *h64, *t64, *stv, *part, *tick;
-    const size_t v32 = stride * sizeof(float2), v64 = stride * sizeof(double2);
+    typedef typename LF::real Rs;
+    typedef typename SpinorT<Rs>::elem E;
+    const size_t v32 = stride * sizeof(E), v64 = stride * sizeof(double2);
     CK(c->ws.get("rb_xs", NR * v32, &xs));
     CK(c->ws.get("rb_rs", NR * v32, &rs));
     CK(c->ws.get("rb_p", NR * v32, &p));
@@ -280,7 +290,7 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     h0.nsys = NR;
     h0.first = 1;
     h0.any_pending = 1;
-    h0.delta2 = 0.05 * 0.05;
+    h0.delta2 = ru_delta * ru_delta;
     h0.ru_max = 2000;
     for (int j = 0; j < NR; j++) {
         h0.tgt[j] = tgt[j];
@@ -301,15 +311,14 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     d1.run_if = &st->any_pending;
     DslashArgs<L64_18, NR, NoFin> d2 = d1;
     d2.p_out = 0; d2.in = (const double2 *)h64; d2.out = (double2 *)t64; d2.beta = -0.5;
-    // FP32 sloppy operator
-    typedef typename LF::real Rs;
+    // sloppy operator
     DslashArgs<LF, NR, NoFin> s1;
     memset(&s1, 0, sizeof(s1));
-    s1.g = c->g; s1.p_out = 1; s1.links = lf; s1.in = (const float2 *)p; s1.out = (float2 *)h; s1.stride = stride;
+    s1.g = c->g; s1.p_out = 1; s1.links = lf; s1.in = (const E *)p; s1.out = (E *)h; s1.stride = stride;
     s1.beta = (Rs)0.5; s1.stop = &st->stop;
     DslashArgs<LF, NR, FinRBAlpha<NR>> s2;
     memset(&s2, 0, sizeof(s2));
-    s2.g = c->g; s2.p_out = 0; s2.links = lf; s2.in = (const float2 *)h; s2.out = (float2 *)ap; s2.y = (const float2 *)p;
+    s2.g = c->g; s2.p_out = 0; s2.links = lf; s2.in = (const E *)h; s2.out = (E *)ap; s2.y = (const E *)p;
     s2.stride = stride; s2.beta = (Rs)-0.5; s2.use_alphas = 1;
     for (int j = 0; j < NR; j++) s2.alphas[j] = (Rs)coef[j];
     s2.partials = pt; s2.ticket = tk + 1; s2.fin.st = st; s2.stop = &st->stop;
@@ -317,17 +326,16 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     cudaGraph_t graph;
     cudaGraphExec_t exec;
     CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-    rb_accum_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (float2 *)xs, st);
+    rb_accum_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (E *)xs, st);
     dslash_kernel<L64_18, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(d1);
     dslash_kernel<L64_18, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(d2);
-    rb_resid_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, bg, xg, (const double2 *)t64, (float2 *)rs, (float2 *)p, co,
+    rb_resid_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, bg, xg, (const double2 *)t64, (E *)rs, (E *)p, co,
                                                          pt, tk, st);
     for (int it = 0; it < n_ru; it++) {
         dslash_kernel<LF, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(s1);
         dslash_kernel<LF, NR, true, true, FinRBAlpha<NR>><<<gd, DSLASH_BLOCK, 0, s_>>>(s2);
-        rb_xr_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (float2 *)xs, (float2 *)rs, (const float2 *)p,
-                                                          (const float2 *)ap, pt, tk + 2, st);
-        rb_p_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const float2 *)rs, (float2 *)p, st);
+        rb_xr_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)xs, (E *)rs, (const E *)p, (const E *)ap, pt, tk + 2, st);
+        rb_p_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)rs, (E *)p, st);
     }
     cudaError_t ce = cudaStreamEndCapture(s_, &graph);
     if (ce != cudaSuccess) return cuda_fail(ce, "refine capture");
@@ -380,14 +388,14 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
 
 template <class LF>
 static int rb_group_n(rhmc_ctx *c, const LF &lf, int n, const double *coef, const double *tgt, double2 *xg, const double2 *bg,
-                      int max_iter, int n_ru, long *iters, int *ru)
+                      int max_iter, int n_ru, long *iters, int *ru, double ru_delta)
 {
     switch (n) {
-    case 1: return rb_group<LF, 1>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
-    case 2: return rb_group<LF, 2>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
-    case 3: return rb_group<LF, 3>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
-    case 4: return rb_group<LF, 4>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
-    case 8: return rb_group<LF, 8>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru);
+    case 1: return rb_group<LF, 1>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru, ru_delta);
+    case 2: return rb_group<LF, 2>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru, ru_delta);
+    case 3: return rb_group<LF, 3>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru, ru_delta);
+    case 4: return rb_group<LF, 4>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru, ru_delta);
+    case 8: return rb_group<LF, 8>(c, lf, coef, tgt, xg, bg, max_iter, n_ru, iters, ru, ru_delta);
     default: return fail(RHMC_ERR_ARG, "bad refinement batch %d", n);
     }
 }
@@ -395,21 +403,24 @@ static int rb_group_n(rhmc_ctx *c, const LF &lf, int n, const double *coef, cons
 // Refine all (rhs, shift) systems of x (FP64 internal [nrhs][nshift]) to |b - A_sigma x| <= res.
 template <class LF>
 static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shifts, int nrhs, double res, int max_iter,
-                      double2 *x, const double2 *b, long *iters, int *ru)
+                      double2 *x, const double2 *b, long *iters, int *ru, double ru_delta, int max_batch = RB_MAX,
+                      const double *skip_below = nullptr)
 {
     const size_t stride = 3 * (size_t)c->Vh;
     const size_t v64 = stride * sizeof(double2);
     void *xg, *bg;
     CK(c->ws.get("rb_xg", RB_MAX * v64, &xg));
     CK(c->ws.get("rb_bg", RB_MAX * v64, &bg));
-    std::vector<int> order(nshift * nrhs);
-    for (int q = 0; q < nshift * nrhs; q++) order[q] = q;
+    std::vector<int> order;
+    for (int q = 0; q < nshift * nrhs; q++)
+        if (!skip_below || skip_below[q] > res) order.push_back(q);
     std::stable_sort(order.begin(), order.end(), [&](int a, int bq) { return shifts[a % nshift] < shifts[bq % nshift]; });
     const double m2 = c->mass * c->mass;
     size_t g0 = 0;
     while (g0 < order.size()) {
         const size_t left = order.size() - g0;
-        const int n = left >= 8 ? 8 : (left >= 4 ? 4 : (int)left);  // instantiated batch widths
+        int n = left >= 8 ? 8 : (left >= 4 ? 4 : (int)left);  // instantiated batch widths
+        if (n > max_batch) n = max_batch;
         double coef[RB_MAX], tgt[RB_MAX];
         for (int j = 0; j < n; j++) {
             const int q = order[g0 + j];
@@ -422,7 +433,7 @@ static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shift
         // iterations between reliable-update stages (systems that need none skip the stage)
         const double kappa = (16.0 + coef[0]) / coef[0];
         const int n_ru = kappa > 1e3 ? 16 : 8;
-        int rc = rb_group_n(c, lf, n, coef, tgt, (double2 *)xg, (const double2 *)bg, max_iter, n_ru, iters, ru);
+        int rc = rb_group_n(c, lf, n, coef, tgt, (double2 *)xg, (const double2 *)bg, max_iter, n_ru, iters, ru, ru_delta);
         if (rc) return rc;
         for (int j = 0; j < n; j++) {
             const int q = order[g0 + j];
@@ -434,60 +445,76 @@ static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shift
 }
 
 int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrhs, double res, int max_iter, double tolA,
-                 double2 *x, const double2 *b, rhmc_msolve_info *info)
+                 double ru_delta, double2 *x, const double2 *b, rhmc_msolve_info *info)
 {
-    if (fmt != RHMC_LINKS_F32_18 && fmt != RHMC_LINKS_F32_12) return fail(RHMC_ERR_ARG, "mixed mode needs an FP32 link format");
     const size_t stride = 3 * (size_t)c->Vh;
     auto t0 = std::chrono::steady_clock::now();
-    // |b_r|^2
-    std::vector<double> b2(nrhs);
-    {
-        void *z;
-        CK(c->ws.get("mx_zero", stride * sizeof(double2), &z));
-        CK(cudaMemsetAsync(z, 0, stride * sizeof(double2), c->stream));
-        const double s0 = 0.0;
-        for (int r = 0; r < nrhs; r++) {
-            int rc = true_residuals(c, 1, &s0, 1, (const double2 *)z, b + r * stride, &b2[r]);
-            if (rc) return rc;
-        }
-    }
-    double bmax = 0;
-    for (double v : b2) bmax = std::max(bmax, std::sqrt(v));
     double smin = shifts[0];
     for (int i = 1; i < nshift; i++) smin = std::min(smin, shifts[i]);
-    std::vector<double> tgt(nshift, std::max(res, tolA * bmax));
-    void *xa;
-    CK(c->ws.get("mx_xa", (size_t)nrhs * nshift * stride * sizeof(float2), &xa));
     MSolveArgs A;
     A.nshift = nshift;
     A.nrhs = nrhs;
     A.shift = shifts;
     A.base_shift = smin;
-    A.tgt = tgt.data();
-    A.res_base = std::max(res, tolA * bmax);
     A.max_iter = max_iter;
     A.stop_on_frozen = 1;
     A.chunk = 8;
     A.b = b;
-    A.x = xa;
     MSolveInfo mi;
     memset(&mi, 0, sizeof(mi));
-    int rc = msolve_shifted(c, fmt, A, &mi);
-    if (rc && rc != RHMC_ERR_MAXITER) return rc;
-    const long n = (long)nrhs * nshift * stride;
-    convert_kernel<float2><<<grid_for(n, 256), 256, 0, c->stream>>>(n, x, (const float2 *)xa);
-    c->launches++;
-    CK(cudaGetLastError());
+    std::vector<double> tgt(nshift);
+    std::vector<double> tr;  // FP64 true residuals after phase A (FP64 phase A only)
+    int rc;
+    const bool f64a = fmt_is_f64(fmt);
+    if (f64a) {
+        // Phase A in FP64 (compressed links when fmt is 12-real), straight into x
+        for (double &t : tgt) t = res;
+        A.tgt = tgt.data();
+        A.res_base = res;
+        A.x = x;
+        rc = msolve_shifted(c, fmt, A, &mi);
+        if (rc && rc != RHMC_ERR_MAXITER) return rc;
+        tr.resize((size_t)nshift * nrhs);
+        rc = true_residuals(c, nshift, shifts, nrhs, x, b, tr.data());
+        if (rc) return rc;
+        for (double &v : tr) v = std::sqrt(v);
+    } else {
+        // Phase A in FP32 to tol_A |b|, then every system is refined
+        std::vector<double> b2(nrhs);
+        void *z;
+        CK(c->ws.get("mx_zero", stride * sizeof(double2), &z));
+        CK(cudaMemsetAsync(z, 0, stride * sizeof(double2), c->stream));
+        const double s0 = 0.0;
+        for (int r = 0; r < nrhs; r++) {
+            rc = true_residuals(c, 1, &s0, 1, (const double2 *)z, b + r * stride, &b2[r]);
+            if (rc) return rc;
+        }
+        double bmax = 0;
+        for (double v : b2) bmax = std::max(bmax, std::sqrt(v));
+        for (double &t : tgt) t = std::max(res, tolA * bmax);
+        void *xa;
+        CK(c->ws.get("mx_xa", (size_t)nrhs * nshift * stride * sizeof(float2), &xa));
+        A.tgt = tgt.data();
+        A.res_base = std::max(res, tolA * bmax);
+        A.x = xa;
+        rc = msolve_shifted(c, fmt, A, &mi);
+        if (rc && rc != RHMC_ERR_MAXITER) return rc;
+        const long n = (long)nrhs * nshift * stride;
+        convert_kernel<float2><<<grid_for(n, 256), 256, 0, c->stream>>>(n, x, (const float2 *)xa);
+        c->launches++;
+        CK(cudaGetLastError());
+    }
     long it_b = 0;
     int ru = 0;
-    if (fmt == RHMC_LINKS_F32_12) {
-        L32_12 lf;
-        links_f32_12(c, &lf);
-        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru);
-    } else {
+    // refinement: FP32 sloppy links of the matching width
+    if (fmt == RHMC_LINKS_F32_18 || fmt == RHMC_LINKS_F64_18) {
         L32_18 lf;
         links_f32_18(c, &lf);
-        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru);
+        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX, tr.empty() ? nullptr : tr.data());
+    } else {
+        L32_12 lf;
+        links_f32_12(c, &lf);
+        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX, tr.empty() ? nullptr : tr.data());
     }
     CK(cudaStreamSynchronize(c->stream));
     if (info) {
@@ -533,10 +560,24 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, con
         if (rc) break;
         done += n;
     }
+    long it_b = 0;
+    int ru = 0;
+    if (rc == RHMC_OK && P->certify) {
+        // FP64 defect correction of every system whose FP64 true residual is above target
+        std::vector<double> tr((size_t)P->nshift * P->nrhs);
+        rc = true_residuals(c, P->nshift, P->shifts, P->nrhs, x, b, tr.data());
+        for (double &v : tr) v = std::sqrt(v);
+        if (rc == RHMC_OK) {
+            L64_18 lf;
+            links_f64_18(c, &lf);
+            rc = refine_all(c, lf, P->nshift, P->shifts, P->nrhs, P->residual, P->max_iter, x, b, &it_b, &ru, 0.05, 1, tr.data());
+        }
+        cudaStreamSynchronize(c->stream);
+    }
     if (info) {
         info->status = rc;
-        info->refine_iters = 0;
-        info->reliable_updates = 0;
+        info->refine_iters = it_b;
+        info->reliable_updates = ru;
         info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
     return rc;
@@ -611,8 +652,9 @@ int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const doubl
         const int nr = P->nrhs;
         if (!(nr == 1 || nr == 2 || nr == 3 || nr == 4 || nr == 8)) return fail(RHMC_ERR_ARG, "mixed mode nrhs must be 1,2,3,4 or 8");
         const double tolA = P->tol_phase_a > 0 ? P->tol_phase_a : 3e-6;
-        return msolve_mixed(c, P->fmt, P->nshift, P->shifts, nr, P->residual, P->max_iter, tolA, (double2 *)x, (const double2 *)b,
-                            info);
+        const double rud = (P->ru_delta > 0 && P->ru_delta < 1) ? P->ru_delta : 0.05;
+        return msolve_mixed(c, P->fmt, P->nshift, P->shifts, nr, P->residual, P->max_iter, tolA, rud, (double2 *)x,
+                            (const double2 *)b, info);
     }
     return fail(RHMC_ERR_ARG, "bad solver mode %d", P->mode);
 }

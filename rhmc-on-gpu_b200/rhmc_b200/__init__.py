@@ -169,6 +169,9 @@ class Context:
     def dslash(self, fmt, parity_out, out, inp, n=1):
         self.call("rhmc_dslash", fmt, parity_out, out, inp, n)
 
+    def dslash_repeat(self, fmt, even, odd, n=1, repeats=1):
+        self.call("rhmc_dslash_repeat", fmt, even, odd, n, repeats)
+
     def dslash_host(self, parity_out, out, inp):
         self.call("rhmc_dslash_host", parity_out, out, inp)
 
@@ -182,7 +185,7 @@ MSOLVE_FP64, MSOLVE_MIXED, MSOLVE_FP32 = 0, 1, 2
 class MsolveParams(ctypes.Structure):
     _fields_ = [("nshift", ctypes.c_int), ("shifts", ctypes.POINTER(ctypes.c_double)), ("nrhs", ctypes.c_int),
                 ("residual", ctypes.c_double), ("max_iter", ctypes.c_int), ("mode", ctypes.c_int), ("fmt", ctypes.c_int),
-                ("tol_phase_a", ctypes.c_double)]
+                ("tol_phase_a", ctypes.c_double), ("ru_delta", ctypes.c_double), ("certify", ctypes.c_int)]
 
 
 class MsolveInfo(ctypes.Structure):
@@ -194,30 +197,32 @@ class MsolveInfo(ctypes.Structure):
                 "reliable_updates": self.reliable_updates, "seconds": self.seconds}
 
 
-def _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a=0.0):
+def _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a=0.0, certify=0, ru_delta=0.0):
     sh = np.ascontiguousarray(shifts, np.float64)
     p = MsolveParams(len(sh), sh.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nrhs, residual, max_iter, mode, fmt,
-                     tol_phase_a)
+                     tol_phase_a, ru_delta, certify)
     p._keep = sh
     return p
 
 
-def _ctx_msolve(self, x, b, shifts, residual, nrhs=1, max_iter=100000, mode=MSOLVE_FP64, fmt=LINKS_F64_18, tol_phase_a=0.0):
+def _ctx_msolve(self, x, b, shifts, residual, nrhs=1, max_iter=100000, mode=MSOLVE_FP64, fmt=LINKS_F64_18, tol_phase_a=0.0,
+                certify=0, ru_delta=0.0):
     """x, b: device FP64 internal spinors (b: nrhs, x: nrhs*nshift, RHS-major)."""
-    p = _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a)
+    p = _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a, certify, ru_delta)
     info = MsolveInfo()
     self.call("rhmc_msolve", ctypes.byref(p), x, b, ctypes.byref(info))
     return info.as_dict()
 
 
-def _ctx_msolve_host(self, b, shifts, residual, max_iter=100000, mode=MSOLVE_FP64, fmt=LINKS_F64_18, tol_phase_a=0.0):
+def _ctx_msolve_host(self, b, shifts, residual, max_iter=100000, mode=MSOLVE_FP64, fmt=LINKS_F64_18, tol_phase_a=0.0,
+                     certify=0):
     """b: numpy complex (Vh,3) or (nrhs,Vh,3) reference layout.  Returns (x, info) with x of shape
     (nshift,Vh,3) or (nrhs,nshift,Vh,3)."""
     b = np.ascontiguousarray(b, np.complex128)
     single = b.ndim == 2
     nrhs = 1 if single else b.shape[0]
     x = np.zeros((nrhs, len(shifts), self.Vh, 3), np.complex128)
-    p = _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a)
+    p = _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a, certify)
     info = MsolveInfo()
     self.call("rhmc_msolve_host", ctypes.byref(p), x, b, ctypes.byref(info))
     return (x[0] if single else x), info.as_dict()
