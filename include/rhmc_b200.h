@@ -162,6 +162,21 @@ int rhmc_msolve_host(rhmc_ctx *ctx, const rhmc_msolve_params *p, double *x, cons
  * The check of inverter.cc:306-338 / cu_inverter.cc:79-120 without the debug build. */
 int rhmc_true_residuals(rhmc_ctx *ctx, int nshift, const double *shifts, int nrhs, const double *x, const double *b, double *out);
 
+/* No counterpart in the reference.  The same values as rhmc_true_residuals, for callers that
+ * cannot allocate device memory where they check their solutions (for example while recording
+ * into a CUDA graph, or under an application-owned memory pool): this entry point takes its
+ * scratch from one fixed device array compiled into the library (RHMC_NOALLOC_SCRATCH_BYTES,
+ * held on every GPU that loads the library until the process exits) and calls no allocator.
+ * Limits: Vh <= RHMC_NOALLOC_MAX_VH sites per parity and nrhs*nshift <= RHMC_NOALLOC_MAX_SYSTEMS;
+ * larger requests return RHMC_ERR_ARG.  The array is shared by all calls on a device: calls whose
+ * GPU work overlaps race.  The first call on a device looks up the array's device address; make
+ * it before any stream capture.  x, b: FP64 internal device spinors; out: host double[nrhs][nshift]. */
+#define RHMC_NOALLOC_MAX_VH 65536
+#define RHMC_NOALLOC_MAX_SYSTEMS 256
+#define RHMC_NOALLOC_SCRATCH_BYTES (2u * 3u * 65536u * 16u + 256u * 8u + 256u * 8u)
+int rhmc_true_residuals_noalloc(rhmc_ctx *ctx, int nshift, const double *shifts, int nrhs, const double *x, const double *b,
+                                double *out);
+
 #ifdef __cplusplus
 }
 #endif
