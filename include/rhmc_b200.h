@@ -162,6 +162,84 @@ int rhmc_msolve_host(rhmc_ctx *ctx, const rhmc_msolve_params *p, double *x, cons
  * The check of inverter.cc:306-338 / cu_inverter.cc:79-120 without the debug build. */
 int rhmc_true_residuals(rhmc_ctx *ctx, int nshift, const double *shifts, int nrhs, const double *x, const double *b, double *out);
 
+/* ------------------------------------------------------------------ forces and updates */
+/* ipdot (=|+ when add) TA((U beta/3) staples): calc_ipdot_gauge (lib/Update/ipdot.cc:25-49) with
+ * calc_staples (lib/Action/staples.cc:16-74); cuda_gauge_deriv (lib/Cuda/cuda_deriv.cu:697-744). */
+int rhmc_gauge_force(rhmc_ctx *ctx, int add);
+/* ipdot (=|+ when add) TA(U F), F = sum over rhs r and shift i of numerators[i] times the outer
+ * products of fermionforce (lib/Action/fermionforce.cc:46-104) built from x_{r,i} and Doe x_{r,i};
+ * cuda_fermion_force (lib/Cuda/cuda_fermion_force.cu:346-418).  x: FP64 internal device spinors
+ * [nrhs][nshift]; numerators: host double[nshift] (rescaled RA_a). */
+int rhmc_fermion_force(rhmc_ctx *ctx, int nrhs, int nshift, const double *numerators, const double *x, int add);
+/* P += i step ipdot: momenta_sum_multiply(i step) (lib/Update/momenta.cc:82-115); cuda_momenta_sum_multiply. */
+int rhmc_mom_update(rhmc_ctx *ctx, double step);
+/* U <- exp(i step P) U, unitarised with the phases: conf_left_exp_multiply(i step)
+ * (lib/Update/momenta.cc:42-78, Su3::exp su3.cc:187-219, unitarize_with_eta conf.cc:235-251);
+ * cuda_exp_su3 (lib/Cuda/cuda_exponentiate.cu:783-828), here 6th order and FP64 throughout. */
+int rhmc_link_update(rhmc_ctx *ctx, double step);
+/* sum_x sum_{mu<nu} beta/3 ReTr(plaquette) (Conf::loc_action, lib/Action/action.cc:6-61). */
+int rhmc_gauge_action(rhmc_ctx *ctx, double *out);
+/* sum over links of 1/2 Tr P^2 (calc_action, lib/Action/action.cc:122-134). */
+int rhmc_momentum_action(rhmc_ctx *ctx, double *out);
+/* spatial and temporal plaquette as Conf::calc_plaq (lib/Measurements/gaugemeas.cc:7-65). */
+int rhmc_plaquette(rhmc_ctx *ctx, double *spatial, double *temporal);
+/* sum over n internal FP64 spinors of Re<a, b> (fermion_action, lib/Action/action.cc:65-107). */
+int rhmc_rdot(rhmc_ctx *ctx, const double *a, const double *b, int n, double *out);
+/* out_r = a0 b_r + sum_i a_i x_{r,i} (rationalapprox.cc:300-311; cuda_sol_sum, lib/Cuda/cuda_sol_sum.cu:168-221);
+ * FP64 internal device spinors, a: host double[nshift]. */
+int rhmc_rational_sum(rhmc_ctx *ctx, int nrhs, int nshift, double a0, const double *a, const double *x, const double *b,
+                      double *out);
+
+/* ------------------------------------------------------------------ molecular-dynamics driver */
+/* Integrators: the reference's use_multistep values (parameters.h:48, update.cc:29-43) plus the
+ * leapfrog of leapfrog.cc with the kick sign of the wired integrators. */
+enum { RHMC_INT_2MN = 0, RHMC_INT_MULTISTEP_2MN = 1, RHMC_INT_MULTISTEP_4MN = 2, RHMC_INT_LEAPFROG = 3 };
+
+typedef struct {
+    int no_flavours;      /* parameters.h:14 */
+    int no_ps;            /* pseudofermions, parameters.h:58 */
+    int no_md;            /* MD steps per unit trajectory, parameters.h:47 */
+    int gauge_scale;      /* gauge steps per fermion step in the multistep integrators, parameters.h:49 */
+    int integrator;       /* RHMC_INT_* */
+    int max_cg;           /* parameters.h:57 */
+    double residue_metro; /* heatbath and action solves, parameters.h:68 */
+    double residue_md;    /* force solves, parameters.h:73 */
+    int metro_mode, metro_fmt; /* RHMC_MSOLVE_* and link format of the heatbath/action solves */
+    int md_mode, md_fmt;       /* ... of the force solves */
+} rhmc_driver_params;
+
+/* Configures the driver of lib/Update (update.cc, ipdot.cc, momenta.cc, MD_integrators). */
+int rhmc_driver_setup(rhmc_ctx *ctx, const rhmc_driver_params *p);
+/* Normalised rational approximation on [min_eps, 1] (RationalApprox, rationalapprox.h:13-47):
+ * which = 0 first (heatbath, x^(N_f/(8 N_ps))), 1 md (force), 2 last (action) (x^(-N_f/(4 N_ps))).
+ * The coefficients rationalapprox_calc (rationalapprox_calc.cc:8-177) would compute at start-up. */
+int rhmc_set_approx(rhmc_ctx *ctx, int which, int order, double a0, const double *a, const double *b, double min_eps);
+/* Spectral bounds of M^dag M that findminmax would return (findminmax.cc:140-183); the rescaling
+ * widens them by 0.95 / 1.05 like RationalApprox::*_inv_approx_coeff (rationalapprox.cc:134-266). */
+int rhmc_set_eig_bounds(rhmc_ctx *ctx, double min, double max);
+/* Pseudofermions phi and chi, reference layout complex[no_ps][Vh][3] (MultiFermion). */
+int rhmc_set_phi(rhmc_ctx *ctx, const double *phi, int location);
+int rhmc_get_phi(rhmc_ctx *ctx, double *phi, int location);
+int rhmc_set_chi(rhmc_ctx *ctx, const double *chi, int location);
+int rhmc_get_chi(rhmc_ctx *ctx, double *chi, int location);
+/* chi = r_first(M^dag M) phi / phi = r_last(M^dag M) chi (rationalapprox.cc:269-369). */
+int rhmc_first_inv_approx_calc(rhmc_ctx *ctx, double res);
+int rhmc_last_inv_approx_calc(rhmc_ctx *ctx, double res);
+/* calc_ipdot, calc_ipdot_gauge, calc_ipdot_fermion (lib/Update/ipdot.cc:25-196). */
+int rhmc_calc_ipdot(rhmc_ctx *ctx);
+int rhmc_calc_ipdot_gauge(rhmc_ctx *ctx);
+int rhmc_calc_ipdot_fermion(rhmc_ctx *ctx);
+/* One MD trajectory with the configured integrator (update_nometro, update.cc:17-53). */
+int rhmc_update_nometro(rhmc_ctx *ctx);
+/* One RHMC trajectory (update, update.cc:58-152) from the momenta and phi set by the caller:
+ * heatbath, initial action, integration, action solve, final action, Metropolis against
+ * `uniform`; *acc = 1 accepted / 0 rejected (configuration restored), *delta_s = S_new - S_old. */
+int rhmc_update(rhmc_ctx *ctx, double uniform, int *acc, double *delta_s);
+/* Conf::save / Conf::copy_saved (lib/Main/Conf/conf.cc:104-140). */
+int rhmc_save_conf(rhmc_ctx *ctx);
+int rhmc_copy_saved(rhmc_ctx *ctx);
+int rhmc_driver_stats(rhmc_ctx *ctx, long *force_evals, long *solves);
+
 /* No counterpart in the reference.  The same values as rhmc_true_residuals, for callers that
  * cannot allocate device memory where they check their solutions (for example while recording
  * into a CUDA graph, or under an application-owned memory pool): this entry point takes its

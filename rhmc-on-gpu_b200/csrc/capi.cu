@@ -71,6 +71,7 @@ int rhmc_create(const rhmc_params *p, rhmc_ctx **out)
     for (int i = 0; i < 4; i++) c->derived_valid[i] = false;
     c->launches = 0;
     c->hflags = nullptr;
+    c->driver = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaHostAlloc((void **)&c->hflags, 256, cudaHostAllocDefault);
     c->aux = nullptr;
@@ -100,6 +101,7 @@ int rhmc_destroy(rhmc_ctx *c)
     cudaFree(c->U64); cudaFree(c->U64_12); cudaFree(c->U32_18); cudaFree(c->U32_12);
     cudaFree(c->P); cudaFree(c->IP);
     c->ws.release();
+    driver_free(c->driver);
     if (c->hflags) cudaFreeHost(c->hflags);
     if (c->aux) {
         cudaStreamDestroy(c->aux);

@@ -14,6 +14,8 @@
 
 namespace rhmc {
 
+struct Driver;
+
 struct Workspace {
     std::map<std::string, std::pair<void *, size_t>> buf;
     cudaError_t get(const std::string &name, size_t bytes, void **out)
@@ -60,6 +62,7 @@ struct rhmc_ctx {
     cudaStream_t aux;
     cudaEvent_t ev_fork, ev_join;
     long launches;  // kernels launched by this context (counted by the host wrappers)
+    rhmc::Driver *driver;  // molecular-dynamics driver state (rhmc_driver_setup), or null
 };
 
 namespace rhmc {
@@ -70,6 +73,7 @@ cudaError_t links_f32_18(rhmc_ctx *c, L32_18 *lf);
 cudaError_t links_f32_12(rhmc_ctx *c, L32_12 *lf);
 void invalidate_links(rhmc_ctx *c);
 int grid_for(long n, int block);
+void driver_free(Driver *d);
 
 // Work issued on c->aux between the constructor and the destructor is ordered after
 // everything already on c->stream and before anything issued on it later.

@@ -1,0 +1,445 @@
+// driver.cu -- the molecular-dynamics driver of lib/Update on device-resident fields.
+//
+// Mirrors, with the same steps and coefficients:
+//   first/last_inv_approx_calc   lib/Tools/RationalApprox/rationalapprox.cc:134-369 (rescale by the
+//                                eigenvalue bounds, shifted solve, chi = a0 phi + sum a_i x_i)
+//   fermionforce / calc_ipdot*   lib/Action/fermionforce.cc:10-110, lib/Update/ipdot.cc:25-196
+//   minimum_norm2_A              lib/Update/MD_integrators/minimum_norm2.cc:28-105
+//   multistep_2MN(_gauge)        multistep_2MN.cc:31-168
+//   multistep_4MN(_gauge)        multistep_4MN.cc:30-300
+//   leapfrog                     leapfrog.cc:18-62, with the momentum kick sign of the wired
+//                                integrators (-i eps); the reference kicks with +i eps, a sign no
+//                                reachable code path uses (update.cc:29-43)
+//   update / update_nometro      lib/Update/update.cc:17-152 with the momenta, the pseudofermions and
+//                                the Metropolis uniform supplied by the caller instead of drawn
+//                                from the host RNG
+// The eigenvalue bounds that findminmax would compute (findminmax.cc:140-183) are supplied by
+// the caller (rhmc_set_eig_bounds); they are widened by 0.95/1.05 as the reference does.
+// Fields stay on the device for the whole trajectory; nothing is reallocated per trajectory.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "capi_util.h"
+#include "context.h"
+#include "kernels.h"
+#include "solver.h"
+
+namespace rhmc {
+
+int gauge_force(rhmc_ctx *c, int mode);
+int fermion_force(rhmc_ctx *c, int nrhs, int nshift, const double *a, const double2 *x, int mode);
+int mom_update(rhmc_ctx *c, double step);
+int link_update(rhmc_ctx *c, double step);
+int plaquette_sums(rhmc_ctx *c, double *temporal, double *spatial);
+int momentum_action(rhmc_ctx *c, double *out);
+int rdot(rhmc_ctx *c, const double2 *a, const double2 *b, long n, double *out);
+int rational_sum(rhmc_ctx *c, int nrhs, int nshift, double a0, const double *a, const double2 *x, const double2 *b, double2 *out);
+
+struct Approx {
+    int order = 0;
+    double a0 = 0, min_eps = 1;
+    std::vector<double> a, b;
+};
+
+struct Driver {
+    rhmc_driver_params P;
+    bool configured = false;
+    Approx approx[3];  // first (heatbath), md (force), last (action); normalised on [min_eps, 1]
+    double eig_min = 0, eig_max = 0;
+    bool have_bounds = false;
+    long force_evals = 0, solves = 0;
+};
+
+static Driver *drv(rhmc_ctx *c) { return c->driver; }
+
+void driver_free(Driver *d) { delete d; }
+
+static size_t SP(rhmc_ctx *c) { return 3 * (size_t)c->Vh; }
+
+static int field(rhmc_ctx *c, const char *name, size_t n_spinors, double2 **out)
+{
+    void *p;
+    CK(c->ws.get(name, n_spinors * SP(c) * sizeof(double2), &p));
+    *out = (double2 *)p;
+    return RHMC_OK;
+}
+
+// RationalApprox::*_inv_approx_coeff (rationalapprox.cc:134-266)
+static Approx rescaled(rhmc_ctx *c, int which)
+{
+    Driver *d = drv(c);
+    Approx r = d->approx[which];
+    const double mx = d->eig_max * 1.05;
+    const double ex = which == 0 ? ((double)d->P.no_flavours) / 8. / ((double)d->P.no_ps)
+                                 : -((double)d->P.no_flavours) / 4. / ((double)d->P.no_ps);
+    const double e = pow(mx, ex);
+    r.a0 *= e;
+    for (int i = 0; i < r.order; i++) {
+        r.a[i] *= (mx * e);
+        r.b[i] *= mx;
+    }
+    return r;
+}
+
+static int solve(rhmc_ctx *c, const Approx &ap, double res, int mode, int fmt, const double2 *b, double2 *x)
+{
+    Driver *d = drv(c);
+    rhmc_msolve_params mp;
+    memset(&mp, 0, sizeof(mp));
+    mp.nshift = ap.order;
+    mp.shifts = ap.b.data();
+    mp.nrhs = d->P.no_ps;
+    mp.residual = res;
+    mp.max_iter = d->P.max_cg;
+    mp.mode = mode;
+    mp.fmt = fmt;
+    d->solves++;
+    return rhmc_msolve(c, &mp, (double *)x, (const double *)b, nullptr);
+}
+
+static int check_ready(rhmc_ctx *c)
+{
+    Driver *d = drv(c);
+    if (!d || !d->configured) return fail(RHMC_ERR_STATE, "driver not configured (rhmc_driver_setup)");
+    if (!d->have_bounds) return fail(RHMC_ERR_STATE, "eigenvalue bounds not set (rhmc_set_eig_bounds)");
+    for (int w = 0; w < 3; w++)
+        if (d->approx[w].order < 1) return fail(RHMC_ERR_STATE, "rational approximation %d not set (rhmc_set_approx)", w);
+    return RHMC_OK;
+}
+
+// chi = r_first(M^dag M) phi (first_inv_approx_calc) or phi = r_last(M^dag M) chi (last_...)
+static int inv_approx_calc(rhmc_ctx *c, int which, double res)
+{
+    int rc = check_ready(c);
+    if (rc) return rc;
+    Driver *d = drv(c);
+    const Approx ap = rescaled(c, which);
+    double2 *phi, *chi, *xs;
+    if ((rc = field(c, "drv_phi", d->P.no_ps, &phi))) return rc;
+    if ((rc = field(c, "drv_chi", d->P.no_ps, &chi))) return rc;
+    if ((rc = field(c, "drv_x", (size_t)d->P.no_ps * ap.order, &xs))) return rc;
+    const double2 *in = which == 0 ? phi : chi;
+    double2 *out = which == 0 ? chi : phi;
+    rc = solve(c, ap, res, d->P.metro_mode, d->P.metro_fmt, in, xs);
+    if (rc) return rc;
+    return rational_sum(c, d->P.no_ps, ap.order, ap.a0, ap.a.data(), xs, in, out);
+}
+
+// calc_ipdot_fermion (overwrite) or its part of calc_ipdot (add)
+static int fermion_part(rhmc_ctx *c, int add)
+{
+    int rc = check_ready(c);
+    if (rc) return rc;
+    Driver *d = drv(c);
+    const Approx ap = rescaled(c, 1);
+    double2 *chi, *xs;
+    if ((rc = field(c, "drv_chi", d->P.no_ps, &chi))) return rc;
+    if ((rc = field(c, "drv_x", (size_t)d->P.no_ps * ap.order, &xs))) return rc;
+    rc = solve(c, ap, d->P.residue_md, d->P.md_mode, d->P.md_fmt, chi, xs);
+    if (rc) return rc;
+    d->force_evals++;
+    return fermion_force(c, d->P.no_ps, ap.order, ap.a.data(), xs, add);
+}
+
+static int calc_ipdot_full(rhmc_ctx *c)
+{
+    int rc = gauge_force(c, 0);
+    if (rc) return rc;
+    return fermion_part(c, 1);
+}
+
+// ------------------------------------------------------------------ integrator schedules
+enum Kind { KICK_FULL, KICK_FERMION, KICK_GAUGE, DRIFT };
+struct Step {
+    Kind k;
+    double c;  // P += i c ipdot after computing the force (KICK_*), or U <- exp(i c P) U (DRIFT)
+};
+
+static const double L2MN = 0.1931833275037836;  // Omelyan et al. (minimum_norm2.cc:35)
+static const double T4 = 0.08398315262876693, R4 = 0.2539785108410595, L4 = 0.6822365335719091, M4 = -0.03230286765269967;
+
+static void sched_2MN_A(std::vector<Step> &s, int no_md, double eps)
+{
+    const double epsh = eps * 0.5;
+    s.push_back({DRIFT, eps * L2MN});
+    for (int md = 1; md < no_md; md++) {
+        s.push_back({KICK_FULL, -epsh});
+        s.push_back({DRIFT, eps * (1.0 - 2.0 * L2MN)});
+        s.push_back({KICK_FULL, -epsh});
+        s.push_back({DRIFT, eps * (2.0 * L2MN)});
+    }
+    s.push_back({KICK_FULL, -epsh});
+    s.push_back({DRIFT, eps * (1.0 - 2.0 * L2MN)});
+    s.push_back({KICK_FULL, -epsh});
+    s.push_back({DRIFT, eps * L2MN});
+}
+
+static void sched_leapfrog(std::vector<Step> &s, int no_md, double eps)
+{
+    const double epsh = eps * 0.5;
+    s.push_back({DRIFT, epsh});
+    for (int md = 1; md < no_md; md++) {
+        s.push_back({KICK_FULL, -eps});
+        s.push_back({DRIFT, eps});
+    }
+    s.push_back({KICK_FULL, -eps});
+    s.push_back({DRIFT, epsh});
+}
+
+static void sched_2MN_gauge(std::vector<Step> &s, int gauge_scale, double eps, double scale)
+{
+    const double epsh = eps * 0.5;
+    s.push_back({KICK_GAUGE, -eps * (scale * L2MN)});
+    for (int md = 1; md < gauge_scale; md++) {
+        s.push_back({DRIFT, epsh * scale});
+        s.push_back({KICK_GAUGE, -eps * ((1.0 - 2.0 * L2MN) * scale)});
+        s.push_back({DRIFT, epsh * scale});
+        s.push_back({KICK_GAUGE, -eps * (2.0 * L2MN * scale)});
+    }
+    s.push_back({DRIFT, epsh * scale});
+    s.push_back({KICK_GAUGE, -eps * ((1.0 - 2.0 * L2MN) * scale)});
+    s.push_back({DRIFT, epsh * scale});
+    s.push_back({KICK_GAUGE, -eps * (L2MN * scale)});
+}
+
+static void sched_multistep_2MN(std::vector<Step> &s, int no_md, int gauge_scale, double eps)
+{
+    const double gs = 0.5 / (double)gauge_scale;
+    s.push_back({KICK_FERMION, -eps * L2MN});
+    for (int md = 1; md < no_md; md++) {
+        sched_2MN_gauge(s, gauge_scale, eps, gs);
+        s.push_back({KICK_FERMION, -eps * (1.0 - 2.0 * L2MN)});
+        sched_2MN_gauge(s, gauge_scale, eps, gs);
+        s.push_back({KICK_FERMION, -eps * (2.0 * L2MN)});
+    }
+    sched_2MN_gauge(s, gauge_scale, eps, gs);
+    s.push_back({KICK_FERMION, -eps * (1.0 - 2.0 * L2MN)});
+    sched_2MN_gauge(s, gauge_scale, eps, gs);
+    s.push_back({KICK_FERMION, -eps * L2MN});
+}
+
+static void sched_4MN_gauge(std::vector<Step> &s, int gauge_scale, double eps, double scale)
+{
+    const double epsh = eps * 0.5;
+    const double half = 1.0 - 2.0 * (L4 + T4), mid = 1.0 - 2.0 * (M4 + R4);
+    auto tail = [&]() {
+        s.push_back({DRIFT, eps * (scale * R4)});
+        s.push_back({KICK_GAUGE, -eps * (L4 * scale)});
+        s.push_back({DRIFT, eps * (scale * M4)});
+        s.push_back({KICK_GAUGE, -epsh * (half * scale)});
+        s.push_back({DRIFT, eps * (scale * mid)});
+        s.push_back({KICK_GAUGE, -epsh * (half * scale)});
+        s.push_back({DRIFT, eps * (scale * M4)});
+        s.push_back({KICK_GAUGE, -eps * (L4 * scale)});
+        s.push_back({DRIFT, eps * (scale * R4)});
+    };
+    s.push_back({KICK_GAUGE, -eps * (scale * T4)});
+    for (int md = 1; md < gauge_scale; md++) {
+        tail();
+        s.push_back({KICK_GAUGE, -eps * (2 * scale * T4)});
+    }
+    tail();
+    s.push_back({KICK_GAUGE, -eps * (scale * T4)});
+}
+
+static void sched_multistep_4MN(std::vector<Step> &s, int no_md, int gauge_scale, double eps)
+{
+    const double epsh = eps * 0.5;
+    const double gs = 1.0 / (double)gauge_scale;
+    const double half = 1.0 - 2.0 * (L4 + T4), mid = 1.0 - 2.0 * (M4 + R4);
+    auto body = [&]() {
+        sched_4MN_gauge(s, gauge_scale, eps, R4 * gs);
+        s.push_back({KICK_FERMION, -eps * L4});
+        sched_4MN_gauge(s, gauge_scale, eps, M4 * gs);
+        s.push_back({KICK_FERMION, -epsh * half});
+        sched_4MN_gauge(s, gauge_scale, eps, gs * mid);
+        s.push_back({KICK_FERMION, -epsh * half});
+        sched_4MN_gauge(s, gauge_scale, eps, M4 * gs);
+        s.push_back({KICK_FERMION, -eps * L4});
+        sched_4MN_gauge(s, gauge_scale, eps, R4 * gs);
+    };
+    s.push_back({KICK_FERMION, -eps * T4});
+    for (int md = 1; md < no_md; md++) {
+        body();
+        s.push_back({KICK_FERMION, -eps * (2 * T4)});
+    }
+    body();
+    s.push_back({KICK_FERMION, -eps * T4});
+}
+
+// the two sched_4MN_* tails reproduce the products of the reference, e.g. mid*gs is computed as
+// gs*(1-2(mu+rho)) in the loop body and as (1-2(mu+rho))*gs in the final part; both are exact
+// products of the same two doubles, so the order does not change the value.
+
+static int run_schedule(rhmc_ctx *c, const std::vector<Step> &s)
+{
+    for (const Step &st : s) {
+        int rc = RHMC_OK;
+        switch (st.k) {
+        case KICK_FULL: rc = calc_ipdot_full(c); break;
+        case KICK_FERMION: rc = fermion_part(c, 0); break;
+        case KICK_GAUGE: rc = gauge_force(c, 0); break;
+        case DRIFT: rc = link_update(c, st.c); break;
+        }
+        if (rc) return rc;
+        if (st.k != DRIFT) {
+            rc = mom_update(c, st.c);
+            if (rc) return rc;
+        }
+    }
+    return RHMC_OK;
+}
+
+static int update_nometro(rhmc_ctx *c)
+{
+    int rc = check_ready(c);
+    if (rc) return rc;
+    const rhmc_driver_params &P = drv(c)->P;
+    const double eps = 1.0 / ((double)P.no_md);
+    std::vector<Step> s;
+    switch (P.integrator) {
+    case RHMC_INT_2MN: sched_2MN_A(s, P.no_md, eps); break;
+    case RHMC_INT_MULTISTEP_2MN: sched_multistep_2MN(s, P.no_md, P.gauge_scale, eps); break;
+    case RHMC_INT_MULTISTEP_4MN: sched_multistep_4MN(s, P.no_md, P.gauge_scale, eps); break;
+    case RHMC_INT_LEAPFROG: sched_leapfrog(s, P.no_md, eps); break;
+    default: return fail(RHMC_ERR_ARG, "unknown integrator %d", P.integrator);
+    }
+    return run_schedule(c, s);
+}
+
+// S = gauge + momenta + fermion part (calc_action, lib/Action/action.cc:111-156)
+static int action(rhmc_ctx *c, int final_part, double *out)
+{
+    Driver *d = drv(c);
+    double t, sp, m, f = 0.0;
+    int rc = plaquette_sums(c, &t, &sp);
+    if (rc) return rc;
+    if ((rc = momentum_action(c, &m))) return rc;
+    double2 *phi, *chi;
+    if ((rc = field(c, "drv_phi", d->P.no_ps, &phi))) return rc;
+    if ((rc = field(c, "drv_chi", d->P.no_ps, &chi))) return rc;
+    // initial: sum Re<phi, phi>; final: sum Re<phi, chi> with phi = r_last chi
+    if ((rc = rdot(c, phi, final_part ? chi : phi, (long)d->P.no_ps * SP(c), &f))) return rc;
+    *out = (c->beta / 3.0) * (t + sp) + m + f;
+    return RHMC_OK;
+}
+
+static int save_conf(rhmc_ctx *c)
+{
+    void *p;
+    const size_t bytes = 8 * 9 * (size_t)c->Vh * sizeof(double2);
+    CK(c->ws.get("drv_usave", bytes, &p));
+    CK(cudaMemcpyAsync(p, c->U64, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    return RHMC_OK;
+}
+
+static int copy_saved(rhmc_ctx *c)
+{
+    auto it = c->ws.buf.find("drv_usave");
+    if (it == c->ws.buf.end()) return fail(RHMC_ERR_STATE, "no saved configuration");
+    CK(cudaMemcpyAsync(c->U64, it->second.first, 8 * 9 * (size_t)c->Vh * sizeof(double2), cudaMemcpyDeviceToDevice,
+                       c->stream));
+    invalidate_links(c);
+    return RHMC_OK;
+}
+
+}  // namespace rhmc
+
+using namespace rhmc;
+
+extern "C" {
+
+int rhmc_driver_setup(rhmc_ctx *c, const rhmc_driver_params *p)
+{
+    if (!c || !p) return fail(RHMC_ERR_ARG, "null argument");
+    if (p->no_ps < 1 || p->no_flavours < 1 || p->no_md < 1 || p->gauge_scale < 1 || p->max_cg < 1)
+        return fail(RHMC_ERR_ARG, "no_ps, no_flavours, no_md, gauge_scale and max_cg must be positive");
+    if (p->integrator < 0 || p->integrator > RHMC_INT_LEAPFROG) return fail(RHMC_ERR_ARG, "unknown integrator");
+    if (!c->driver) c->driver = new Driver();
+    c->driver->P = *p;
+    c->driver->configured = true;
+    return RHMC_OK;
+}
+
+int rhmc_set_approx(rhmc_ctx *c, int which, int order, double a0, const double *a, const double *b, double min_eps)
+{
+    if (!c || !a || !b || which < 0 || which > 2 || order < 1 || order > 32) return fail(RHMC_ERR_ARG, "bad argument");
+    if (!c->driver) c->driver = new Driver();
+    Approx &ap = c->driver->approx[which];
+    ap.order = order;
+    ap.a0 = a0;
+    ap.min_eps = min_eps;
+    ap.a.assign(a, a + order);
+    ap.b.assign(b, b + order);
+    return RHMC_OK;
+}
+
+int rhmc_set_eig_bounds(rhmc_ctx *c, double min, double max)
+{
+    if (!c || !(max > 0.0) || !(min > 0.0) || min > max) return fail(RHMC_ERR_ARG, "need 0 < min <= max");
+    if (!c->driver) c->driver = new Driver();
+    c->driver->eig_min = min;
+    c->driver->eig_max = max;
+    c->driver->have_bounds = true;
+    return RHMC_OK;
+}
+
+static int pf_io(rhmc_ctx *c, const char *name, double *host_ref, int location, int to_device)
+{
+    if (!c || !host_ref) return fail(RHMC_ERR_ARG, "null argument");
+    if (!c->driver || !c->driver->configured) return fail(RHMC_ERR_STATE, "driver not configured");
+    const int n = c->driver->P.no_ps;
+    double2 *f;
+    int rc = field(c, name, n, &f);
+    if (rc) return rc;
+    if (to_device) return rhmc_spinor_to_internal(c, RHMC_LINKS_F64_18, f, host_ref, n, location);
+    return rhmc_spinor_from_internal(c, RHMC_LINKS_F64_18, host_ref, f, n, location);
+}
+
+int rhmc_set_phi(rhmc_ctx *c, const double *phi, int location) { return pf_io(c, "drv_phi", (double *)phi, location, 1); }
+int rhmc_get_phi(rhmc_ctx *c, double *phi, int location) { return pf_io(c, "drv_phi", phi, location, 0); }
+int rhmc_set_chi(rhmc_ctx *c, const double *chi, int location) { return pf_io(c, "drv_chi", (double *)chi, location, 1); }
+int rhmc_get_chi(rhmc_ctx *c, double *chi, int location) { return pf_io(c, "drv_chi", chi, location, 0); }
+
+int rhmc_first_inv_approx_calc(rhmc_ctx *c, double res) { return c ? inv_approx_calc(c, 0, res) : fail(RHMC_ERR_ARG, "null"); }
+int rhmc_last_inv_approx_calc(rhmc_ctx *c, double res) { return c ? inv_approx_calc(c, 2, res) : fail(RHMC_ERR_ARG, "null"); }
+int rhmc_calc_ipdot(rhmc_ctx *c) { return c ? calc_ipdot_full(c) : fail(RHMC_ERR_ARG, "null"); }
+int rhmc_calc_ipdot_gauge(rhmc_ctx *c) { return c ? gauge_force(c, 0) : fail(RHMC_ERR_ARG, "null"); }
+int rhmc_calc_ipdot_fermion(rhmc_ctx *c) { return c ? fermion_part(c, 0) : fail(RHMC_ERR_ARG, "null"); }
+int rhmc_update_nometro(rhmc_ctx *c) { return c ? update_nometro(c) : fail(RHMC_ERR_ARG, "null"); }
+int rhmc_save_conf(rhmc_ctx *c) { return c ? save_conf(c) : fail(RHMC_ERR_ARG, "null"); }
+int rhmc_copy_saved(rhmc_ctx *c) { return c ? copy_saved(c) : fail(RHMC_ERR_ARG, "null"); }
+
+int rhmc_update(rhmc_ctx *c, double uniform, int *acc, double *delta_s)
+{
+    if (!c || !acc) return fail(RHMC_ERR_ARG, "null argument");
+    int rc = check_ready(c);
+    if (rc) return rc;
+    Driver *d = drv(c);
+    if ((rc = save_conf(c))) return rc;
+    if ((rc = inv_approx_calc(c, 0, d->P.residue_metro))) return rc;
+    double s0, s1;
+    if ((rc = action(c, 0, &s0))) return rc;
+    if ((rc = update_nometro(c))) return rc;
+    if ((rc = inv_approx_calc(c, 2, d->P.residue_metro))) return rc;
+    if ((rc = action(c, 1, &s1))) return rc;
+    const double de = s1 - s0;
+    if (delta_s) *delta_s = de;
+    if (de < 0 || uniform < exp(-de)) {
+        *acc = 1;
+        return save_conf(c);
+    }
+    *acc = 0;
+    return copy_saved(c);
+}
+
+int rhmc_driver_stats(rhmc_ctx *c, long *force_evals, long *solves)
+{
+    if (!c || !c->driver) return fail(RHMC_ERR_STATE, "driver not configured");
+    if (force_evals) *force_evals = c->driver->force_evals;
+    if (solves) *solves = c->driver->solves;
+    return RHMC_OK;
+}
+
+}  // extern "C"

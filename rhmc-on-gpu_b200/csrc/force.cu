@@ -1,0 +1,183 @@
+// force.cu -- molecular-dynamics forces on sm_100a, FP64.
+//
+// ipdot = TA(U (beta/3 staples + F_f)) (calc_ipdot, lib/Update/ipdot.cc:149-196).  TA is linear,
+// so the gauge part and the fermion part are produced by separate kernels that either
+// overwrite or add into ipdot:
+//   gauge_force_kernel   TA((U beta/3) staples), staples as calc_staples (lib/Action/staples.cc:16-74)
+//   fermion_force_kernel TA(U F_f) with F_f the outer products of fermionforce
+//                        (lib/Action/fermionforce.cc:46-104): even x: sum a_i h_i(x+mu) (x) x_i(x)^*,
+//                        odd x: -sum a_i x_i(x+mu) (x) h_i(x)^*, h_i = Doe x_i (with its 1/2).
+// One thread per link, mu fastest inside a site (the four links of a site share the site's
+// loads through L1).  All shifted solutions of all right-hand sides are summed in registers,
+// so the 18-real force matrix never goes to HBM (the reference GPU code read-modify-writes an
+// 18 x 4V float buffer once per shift, lib/Cuda/cuda_fermion_force.cu:370-386).
+#include <vector>
+
+#include "capi_util.h"
+#include "context.h"
+#include "kernels.h"
+#include "su3.cuh"
+
+namespace rhmc {
+
+constexpr int FORCE_BLOCK = 128;
+
+__device__ __forceinline__ Site shifted(const Geom &g, Site s, int mu, int dir)
+{
+    if (mu == 0) { s.x += dir; s.x = s.x < 0 ? g.nx - 1 : (s.x >= g.nx ? 0 : s.x); }
+    else if (mu == 1) { s.y += dir; s.y = s.y < 0 ? g.ny - 1 : (s.y >= g.ny ? 0 : s.y); }
+    else if (mu == 2) { s.z += dir; s.z = s.z < 0 ? g.nz - 1 : (s.z >= g.nz ? 0 : s.z); }
+    else { s.t += dir; s.t = s.t < 0 ? g.nt - 1 : (s.t >= g.nt ? 0 : s.t); }
+    return s;
+}
+
+__device__ __forceinline__ int hidx(const Geom &g, const Site &s) { return half_index(g, s.x, s.y, s.z, s.t); }
+
+// S_mu(x) = sum_{nu != mu} [ U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
+//                          + U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu) ]
+__device__ M3 staple_sum(const Geom &g, const double2 *__restrict__ U, int mu, int p, const Site &s)
+{
+    const int Vh = g.Vh, q = 1 - p;
+    const Site xpm = shifted(g, s, mu, +1);
+    const int kxpm = hidx(g, xpm), kx = hidx(g, s);
+    M3 S = m3_zero();
+#pragma unroll 1
+    for (int nu = 0; nu < 4; nu++) {
+        if (nu == mu) continue;
+        const Site xpn = shifted(g, s, nu, +1), xmn = shifted(g, s, nu, -1), xpmmn = shifted(g, xpm, nu, -1);
+        M3 a = m3_mul_nd(load_link64(U, Vh, nu, q, kxpm), load_link64(U, Vh, mu, q, hidx(g, xpn)));
+        a = m3_mul_nd(a, load_link64(U, Vh, nu, p, kx));
+        m3_add(S, a);
+        const int kxmn = hidx(g, xmn);
+        const M3 ba = m3_mul(load_link64(U, Vh, mu, q, kxmn), load_link64(U, Vh, nu, p, hidx(g, xpmmn)));
+        m3_add(S, m3_mul_dn(ba, load_link64(U, Vh, nu, q, kxmn)));
+    }
+    return S;
+}
+
+// mode 0: ipdot = TA(U beta/3 S); mode 1: ipdot += TA(U beta/3 S)
+__global__ void __launch_bounds__(FORCE_BLOCK) gauge_force_kernel(Geom g, const double2 *__restrict__ U, double *IP,
+                                                                   double beta_by_three, int mode)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int Vh = g.Vh;
+    if (t >= 8L * Vh) return;
+    const int mu = (int)(t & 3);
+    const long site = t >> 2;
+    const int p = site >= Vh;
+    const int k = (int)(site - (long)p * Vh);
+    const Site s = site_of(g, p, k);
+    const M3 S = staple_sum(g, U, mu, p, s);
+    M3 us = m3_mul(load_link64(U, Vh, mu, p, k), S);
+    m3_scale(us, beta_by_three);
+    double o[8];
+    ta_pack(us, o);
+    if (mode) {
+        double c[8];
+        load_alg(IP, Vh, mu, p, k, c);
+#pragma unroll
+        for (int j = 0; j < 8; j++) o[j] += c[j];
+    }
+    store_alg(IP, Vh, mu, p, k, o);
+}
+
+// x: even FP64 spinors [nv], h = Doe x: odd FP64 spinors [nv]; coef[v] the numerator of vector v
+__global__ void __launch_bounds__(FORCE_BLOCK) fermion_force_kernel(Geom g, const double2 *__restrict__ U,
+                                                                     const double2 *__restrict__ x,
+                                                                     const double2 *__restrict__ h, int nv,
+                                                                     const double *__restrict__ coef, double *IP, int mode)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int Vh = g.Vh;
+    if (t >= 8L * Vh) return;
+    const int mu = (int)(t & 3);
+    const long site = t >> 2;
+    const int p = site >= Vh;
+    const int k = (int)(site - (long)p * Vh);
+    const Site s = site_of(g, p, k);
+    const int kn = neighbour(g, s, mu, +1);  // x+mu, opposite parity
+    const size_t stride = 3 * (size_t)Vh;
+    // even x: a h(x+mu) (x) x(x)^* ; odd x: -a x(x+mu) (x) h(x)^*
+    const double2 *left = p == 0 ? h : x;
+    const double2 *right = p == 0 ? x : h;
+    const int kl = kn, kr = k;
+    const double sgn = p == 0 ? 1.0 : -1.0;
+    M3 F = m3_zero();
+#pragma unroll 2
+    for (int v = 0; v < nv; v++) {
+        const double a = sgn * __ldg(coef + v);
+        const double2 *L = left + v * stride, *R = right + v * stride;
+        C l[3], r[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const double2 lv = __ldg(L + (size_t)c * Vh + kl), rv = __ldg(R + (size_t)c * Vh + kr);
+            l[c] = mk<double>(a * lv.x, a * lv.y);
+            r[c] = mk<double>(rv.x, -rv.y);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) F.e[i][j] = cmadd(l[i], r[j], F.e[i][j]);
+    }
+    const M3 uf = m3_mul(load_link64(U, Vh, mu, p, k), F);
+    double o[8];
+    ta_pack(uf, o);
+    if (mode) {
+        double c[8];
+        load_alg(IP, Vh, mu, p, k, c);
+#pragma unroll
+        for (int j = 0; j < 8; j++) o[j] += c[j];
+    }
+    store_alg(IP, Vh, mu, p, k, o);
+}
+
+int gauge_force(rhmc_ctx *c, int mode)
+{
+    const long n = 8L * c->Vh;
+    gauge_force_kernel<<<grid_for(n, FORCE_BLOCK), FORCE_BLOCK, 0, c->stream>>>(c->g, c->U64, c->IP, c->beta / 3.0, mode);
+    c->launches++;
+    CK(cudaGetLastError());
+    return RHMC_OK;
+}
+
+// x: [nrhs][nshift] FP64 internal even spinors; a: numerators per shift
+int fermion_force(rhmc_ctx *c, int nrhs, int nshift, const double *a, const double2 *x, int mode)
+{
+    const int nv = nrhs * nshift;
+    const size_t stride = 3 * (size_t)c->Vh;
+    void *h, *co;
+    CK(c->ws.get("ff_h", (size_t)nv * stride * sizeof(double2), &h));
+    CK(c->ws.get("ff_coef", (size_t)nv * sizeof(double), &co));
+    std::vector<double> hc(nv);
+    for (int v = 0; v < nv; v++) hc[v] = a[v % nshift];
+    CK(cudaMemcpyAsync(co, hc.data(), nv * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    // h = Doe x for every vector, links read once per batch of up to 8
+    cudaError_t e = launch_dslash(c, RHMC_LINKS_F64_18, 1, h, x, stride, nv, nullptr, 0.0, 0.5, nullptr, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "fermion_force dslash");
+    const long n = 8L * c->Vh;
+    fermion_force_kernel<<<grid_for(n, FORCE_BLOCK), FORCE_BLOCK, 0, c->stream>>>(c->g, c->U64, x, (const double2 *)h, nv,
+                                                                                  (const double *)co, c->IP, mode);
+    c->launches++;
+    CK(cudaGetLastError());
+    return RHMC_OK;
+}
+
+}  // namespace rhmc
+
+using namespace rhmc;
+
+extern "C" {
+
+int rhmc_gauge_force(rhmc_ctx *c, int add)
+{
+    if (!c) return fail(RHMC_ERR_ARG, "null context");
+    return gauge_force(c, add ? 1 : 0);
+}
+
+int rhmc_fermion_force(rhmc_ctx *c, int nrhs, int nshift, const double *numerators, const double *x, int add)
+{
+    if (!c || !numerators || !x || nrhs < 1 || nshift < 1) return fail(RHMC_ERR_ARG, "bad argument");
+    return fermion_force(c, nrhs, nshift, numerators, (const double2 *)x, add ? 1 : 0);
+}
+
+}  // extern "C"

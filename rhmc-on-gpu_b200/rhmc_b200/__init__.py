@@ -238,3 +238,87 @@ def _ctx_true_residuals(self, x, b, shifts, nrhs=1):
 Context.msolve = _ctx_msolve
 Context.msolve_host = _ctx_msolve_host
 Context.true_residuals = _ctx_true_residuals
+
+
+def _f(self, name, *args):
+    v = ctypes.c_double()
+    self.call(name, *args, ctypes.byref(v))
+    return v.value
+
+
+Context.gauge_force = lambda self, add=0: self.call("rhmc_gauge_force", int(add))
+Context.fermion_force = lambda self, x, numerators, nrhs=1, add=0: self.call(
+    "rhmc_fermion_force", nrhs, len(numerators), np.ascontiguousarray(numerators, np.float64), x, int(add))
+Context.mom_update = lambda self, step: self.call("rhmc_mom_update", float(step))
+Context.link_update = lambda self, step: self.call("rhmc_link_update", float(step))
+Context.gauge_action = lambda self: _f(self, "rhmc_gauge_action")
+Context.momentum_action = lambda self: _f(self, "rhmc_momentum_action")
+Context.rdot = lambda self, a, b, n=1: _f(self, "rhmc_rdot", a, b, n)
+
+
+def _plaq(self):
+    s, t = ctypes.c_double(), ctypes.c_double()
+    self.call("rhmc_plaquette", ctypes.byref(s), ctypes.byref(t))
+    return s.value, t.value
+
+
+Context.plaquette = _plaq
+Context.rational_sum = lambda self, out, x, b, a0, a, nrhs=1: self.call(
+    "rhmc_rational_sum", nrhs, len(a), float(a0), np.ascontiguousarray(a, np.float64), x, b, out)
+
+
+INT_2MN, INT_MULTISTEP_2MN, INT_MULTISTEP_4MN, INT_LEAPFROG = 0, 1, 2, 3
+
+
+class DriverParams(ctypes.Structure):
+    _fields_ = [("no_flavours", ctypes.c_int), ("no_ps", ctypes.c_int), ("no_md", ctypes.c_int),
+                ("gauge_scale", ctypes.c_int), ("integrator", ctypes.c_int), ("max_cg", ctypes.c_int),
+                ("residue_metro", ctypes.c_double), ("residue_md", ctypes.c_double),
+                ("metro_mode", ctypes.c_int), ("metro_fmt", ctypes.c_int), ("md_mode", ctypes.c_int),
+                ("md_fmt", ctypes.c_int)]
+
+
+def _driver_setup(self, no_flavours=2, no_ps=1, no_md=10, gauge_scale=5, integrator=INT_2MN, max_cg=100000,
+                  residue_metro=1e-10, residue_md=1e-10, metro_mode=MSOLVE_FP64, metro_fmt=LINKS_F64_18,
+                  md_mode=MSOLVE_FP64, md_fmt=LINKS_F64_18):
+    p = DriverParams(no_flavours, no_ps, no_md, gauge_scale, integrator, max_cg, residue_metro, residue_md, metro_mode,
+                     metro_fmt, md_mode, md_fmt)
+    self.no_ps = no_ps
+    self.call("rhmc_driver_setup", ctypes.byref(p))
+
+
+def _set_approx(self, which, approx):
+    a = np.ascontiguousarray(approx["a"], np.float64)
+    b = np.ascontiguousarray(approx["b"], np.float64)
+    self.call("rhmc_set_approx", which, len(a), float(approx["a0"]), a, b, float(approx.get("min_eps", 1e-7)))
+
+
+def _pf_get(self, name):
+    out = np.zeros((self.no_ps, self.Vh, 3), np.complex128)
+    self.call(name, out, HOST)
+    return out
+
+
+def _update(self, uniform):
+    acc = ctypes.c_int()
+    de = ctypes.c_double()
+    self.call("rhmc_update", float(uniform), ctypes.byref(acc), ctypes.byref(de))
+    return de.value, acc.value
+
+
+Context.driver_setup = _driver_setup
+Context.set_approx = _set_approx
+Context.set_eig_bounds = lambda self, mn, mx: self.call("rhmc_set_eig_bounds", float(mn), float(mx))
+Context.set_phi = lambda self, phi: self.call("rhmc_set_phi", np.ascontiguousarray(phi, np.complex128), HOST)
+Context.set_chi = lambda self, chi: self.call("rhmc_set_chi", np.ascontiguousarray(chi, np.complex128), HOST)
+Context.get_phi = lambda self: _pf_get(self, "rhmc_get_phi")
+Context.get_chi = lambda self: _pf_get(self, "rhmc_get_chi")
+Context.first_inv_approx_calc = lambda self, res: self.call("rhmc_first_inv_approx_calc", float(res))
+Context.last_inv_approx_calc = lambda self, res: self.call("rhmc_last_inv_approx_calc", float(res))
+Context.calc_ipdot = lambda self: self.call("rhmc_calc_ipdot")
+Context.calc_ipdot_gauge = lambda self: self.call("rhmc_calc_ipdot_gauge")
+Context.calc_ipdot_fermion = lambda self: self.call("rhmc_calc_ipdot_fermion")
+Context.update_nometro = lambda self: self.call("rhmc_update_nometro")
+Context.update = _update
+Context.save_conf = lambda self: self.call("rhmc_save_conf")
+Context.copy_saved = lambda self: self.call("rhmc_copy_saved")

@@ -1,0 +1,87 @@
+"""Rational approximations r(x) = a0 + sum_i a_i / (x + b_i) of x^p on [eps, 1].
+
+The reference builds them at start-up with AlgRemez over MPFR (lib/Tools/RationalApprox/
+rationalapprox_calc.cc:8-177, alg_remez.cc) and stores them normalised on [lambda_min, 1] in a
+RationalApprox (rationalapprox.h:13-47); the first/md/last coefficients are then rescaled by the
+largest eigenvalue (rationalapprox.cc:134-266).  MPFR is not available here, so this module
+produces the same object a different way: poles b_i > 0 are placed log-uniformly (the sinc
+quadrature of x^-q = sin(pi q)/pi int_0^inf t^-q/(t+x) dt), the numerators follow from a linear
+least-squares fit of the relative error on a log grid, and the log-poles are then adjusted with
+scipy's least_squares to minimise the relative error, which approaches the minimax (Remez)
+solution.  For 0 < p < 1 the form x * x^(p-1) gives a0 = sum w_i and a_i = -w_i b_i.
+
+The result is returned with its measured maximum relative error on [eps, 1]; the oracle and the
+GPU path read the same numbers, so approximation quality does not affect parity.
+"""
+import numpy as np
+
+
+def _design(x, b, with_a0):
+    cols = [1.0 / (x[:, None] + b[None, :])]
+    if with_a0:
+        cols.insert(0, np.ones((x.size, 1)))
+    return np.hstack(cols)
+
+
+def _fit(x, f, b, with_a0):
+    A = _design(x, b, with_a0) / f[:, None]
+    coef, *_ = np.linalg.lstsq(A, np.ones_like(f), rcond=None)
+    return coef
+
+
+def _eval(x, b, coef, with_a0):
+    return _design(x, b, with_a0) @ coef
+
+
+def inverse_power(q, n, eps, optimise=True, grid=3000):
+    """x^-q (0 < q < 1) on [eps, 1] with n poles: a0 = 0."""
+    x = np.geomspace(eps, 1.0, grid)
+    f = x ** (-q)
+    # sinc-quadrature pole positions: log-uniform a little beyond the interval
+    lo, hi = np.log(eps) - 2.0, np.log(1.0) + 3.0
+    s = np.linspace(lo, hi, n)
+    b = np.exp(s)
+
+    def resid(logb):
+        bb = np.exp(logb)
+        c = _fit(x, f, bb, False)
+        return _eval(x, bb, c, False) / f - 1.0
+
+    if optimise and n > 1:
+        from scipy.optimize import least_squares
+        # keep the poles within a few decades of the interval (a pole running off to infinity
+        # only mimics a constant term and makes a useless solver shift)
+        blo, bhi = np.log(eps) - 6.0, np.log(1.0) + 6.0
+        sol = least_squares(resid, np.clip(s, blo + 1e-9, bhi - 1e-9), bounds=(blo, bhi), method="trf", max_nfev=3000)
+        s = np.sort(sol.x)
+        b = np.exp(s)
+    a = _fit(x, f, b, False)
+    err = np.max(np.abs(_eval(x, b, a, False) / f - 1.0))
+    return 0.0, a, b, err
+
+
+def rational_power(p, n, eps, optimise=True):
+    """Coefficients of x^p on [eps, 1], p in (-1, 0) or (0, 1), degree n.
+    Returns dict(a0, a, b, min_eps, power, max_rel_err)."""
+    if 0.0 < -p < 1.0:
+        a0, a, b, err = inverse_power(-p, n, eps, optimise)
+    elif 0.0 < p < 1.0:
+        # x^p = x * x^(p-1):  x sum w/(x+b) = sum w - sum w b/(x+b)
+        _, w, b, _ = inverse_power(1.0 - p, n, eps, optimise)
+        a0 = float(np.sum(w))
+        a = -w * b
+        x = np.geomspace(eps, 1.0, 3000)
+        r = a0 + (a[None, :] / (x[:, None] + b[None, :])).sum(1)
+        err = float(np.max(np.abs(r / x ** p - 1.0)))
+    else:
+        raise ValueError("power must be in (-1, 0) or (0, 1)")
+    return {"a0": float(a0), "a": [float(v) for v in a], "b": [float(v) for v in b], "min_eps": float(eps),
+            "power": float(p), "max_rel_err": float(err)}
+
+
+def rescale(approx, lam_max, exponent):
+    """The rescaling of RationalApprox::*_inv_approx_coeff (rationalapprox.cc:162-170, 206-214,
+    250-258): with e = lam_max^exponent, a0 -> a0 e, a_i -> a_i lam_max e, b_i -> b_i lam_max.
+    lam_max is the already enlarged bound (the reference multiplies findminmax's max by 1.05)."""
+    e = lam_max ** exponent
+    return {"a0": approx["a0"] * e, "a": [v * lam_max * e for v in approx["a"]], "b": [v * lam_max for v in approx["b"]]}
