@@ -89,10 +89,22 @@ class Context:
         _check(lib().rhmc_create(ctypes.byref(p), ctypes.byref(h)))
         self.h = h
 
+    @classmethod
+    def wrap(cls, handle, dims, mass, beta):
+        """A view of a context owned elsewhere (e.g. the legacy entry points'); never destroyed here."""
+        self = cls.__new__(cls)
+        self.dims = tuple(int(d) for d in dims)
+        self.V = int(np.prod(self.dims))
+        self.Vh = self.V // 2
+        self.mass, self.beta = mass, beta
+        self.h = ctypes.c_void_p(handle)
+        self.owned = False
+        return self
+
     def close(self):
-        if self.h:
+        if self.h and getattr(self, "owned", True):
             lib().rhmc_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -322,3 +334,73 @@ Context.update_nometro = lambda self: self.call("rhmc_update_nometro")
 Context.update = _update
 Context.save_conf = lambda self: self.call("rhmc_save_conf")
 Context.copy_saved = lambda self: self.call("rhmc_copy_saved")
+
+
+class LegacyConfig(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("nt", ctypes.c_int),
+                ("ferm_temp_bc", ctypes.c_int), ("mass", ctypes.c_double), ("beta", ctypes.c_double),
+                ("no_ps", ctypes.c_int), ("max_approx_order", ctypes.c_int), ("max_cg", ctypes.c_int),
+                ("device", ctypes.c_int),
+                ("gauge_field_packed", ctypes.c_void_p), ("chi_packed", ctypes.c_void_p),
+                ("simple_fermion_packed", ctypes.c_void_p), ("ipdot_packed", ctypes.c_void_p),
+                ("momenta_packed", ctypes.c_void_p), ("shift_table", ctypes.c_void_p), ("eta", ctypes.c_void_p)]
+
+
+class Legacy:
+    """The reference's extern "C" GPU entry points (include/rhmc_legacy.h) over host numpy
+    buffers in the packer formats; keeps the buffers alive while bound."""
+
+    def __init__(self, dims, mass, beta, no_ps, max_approx_order, max_cg, buffers, ferm_temp_bc=0, device=0):
+        self.buffers = buffers
+
+        def ptr(k):
+            return ctypes.c_void_p(buffers[k].ctypes.data) if buffers.get(k) is not None else ctypes.c_void_p(None)
+
+        cfg = LegacyConfig(*dims, ferm_temp_bc, mass, beta, no_ps, max_approx_order, max_cg, device,
+                           ptr("gauge_field_packed"), ptr("chi_packed"), ptr("simple_fermion_packed"),
+                           ptr("ipdot_packed"), ptr("momenta_packed"), ptr("shift_table"), ptr("eta"))
+        _check(lib().rhmc_legacy_bind(ctypes.byref(cfg)))
+        L = lib()
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.cuda_shifted_inverter.argtypes = [ctypes.c_double, dp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.cuda_shifted_inverter_d.argtypes = L.cuda_shifted_inverter.argtypes
+        L.cuda_sol_sum.argtypes = [ctypes.c_int, ctypes.c_double, dp]
+        L.cuda_fermion_force.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+        L.cuda_gauge_deriv.argtypes = [ctypes.c_int]
+        L.cuda_exp_su3.argtypes = [ctypes.c_float]
+        L.cuda_momenta_sum_multiply.argtypes = [ctypes.c_float]
+        L.cuda_find_max.argtypes = [dp]
+        L.cuda_find_min.argtypes = [dp, ctypes.c_double]
+        L.rhmc_legacy_context.restype = ctypes.c_void_p
+        self.L = L
+
+    def context_handle(self):
+        return self.L.rhmc_legacy_context()
+
+    def shifted_inverter(self, res, shifts, psferm, double=True):
+        sh = np.ascontiguousarray(shifts, np.float64)
+        n = ctypes.c_int()
+        f = self.L.cuda_shifted_inverter_d if double else self.L.cuda_shifted_inverter
+        f(res, sh.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(sh), psferm, ctypes.byref(n))
+        return n.value
+
+    def sol_sum(self, a0, a):
+        a = np.ascontiguousarray(a, np.float64)
+        self.L.cuda_sol_sum(len(a), a0, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+
+    def fermion_force(self, a):
+        a = np.ascontiguousarray(a, np.float32)
+        self.L.cuda_fermion_force(len(a), a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+
+    def find_max(self):
+        v = ctypes.c_double()
+        self.L.cuda_find_max(ctypes.byref(v))
+        return v.value
+
+    def find_min(self, mx):
+        v = ctypes.c_double()
+        self.L.cuda_find_min(ctypes.byref(v), mx)
+        return v.value
+
+    def __getattr__(self, name):  # cuda_init0, cuda_init1, cuda_end, cuda_gauge_deriv, ...
+        return getattr(self.L, name)
