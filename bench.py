@@ -194,6 +194,7 @@ MS_DIMS = (24, 24, 24, 32)
 
 
 def msolve_bench(rb, F, np, torch, rank, dev, stream, nrhs=4, nshift=16, res=1e-10):
+    from rhmc_b200 import replicas as RP
     """Multi-shift CG at 24^3x32, am=0.01: 16 poles log-spaced in [1e-4, 50], 4 Gaussian RHS,
     true residual 1e-10.  Plain FP64 single-RHS (the reference algorithm, RHS after RHS, then
     FP64 CG refinement of every system whose FP64 true residual is still above 1e-10) against
@@ -201,11 +202,11 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, nrhs=4, nshift=16, res=1e-
     without the refinement is reported too (it stops on its iterated residual)."""
     ctx = rb.Context(MS_DIMS, mass=0.01, beta=5.7, device=dev.index or 0)
     ctx.set_stream(stream.cuda_stream)
-    u = F.random_links(MS_DIMS, seed=1001 + rank)
+    u = F.random_links(MS_DIMS, seed=RP.replica_seed(1001, rank))
     ctx.set_gauge(u)
     Vh = ctx.Vh
     shifts = 1e-4 * (5e5) ** (np.arange(nshift) / (nshift - 1.0))
-    b_host = F.random_spinor(MS_DIMS, seed=2002 + rank, n=nrhs)
+    b_host = F.random_spinor(MS_DIMS, seed=RP.replica_seed(2002, rank), n=nrhs)
     b = torch.zeros(nrhs * 6 * Vh, dtype=torch.float64, device=dev)
     ctx.spinor_to_internal(rb.LINKS_F64_18, b, b_host, nrhs)
     x = torch.zeros(nrhs * nshift * 6 * Vh, dtype=torch.float64, device=dev)
@@ -257,6 +258,7 @@ def main():
     import torch
     import rhmc_b200 as rb
     from rhmc_b200 import fields as F
+    from rhmc_b200 import replicas as RP
 
     global DIMS
     DIMS = tuple(int(v) for v in a.dims.split(","))
@@ -277,9 +279,9 @@ def main():
     ctx = rb.Context(DIMS, mass=0.01, beta=5.8, device=local)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
-    u = F.random_links(DIMS, seed=1001 + rank)
+    u = F.random_links(DIMS, seed=RP.replica_seed(1001, rank))
     ctx.set_gauge(u)
-    x = F.random_spinor(DIMS, seed=2002 + rank)
+    x = F.random_spinor(DIMS, seed=RP.replica_seed(2002, rank))
 
     peak, peak_kind = load_peaks()
 
@@ -288,11 +290,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return RP.max_over_ranks(v, dist, dev)
 
     results = {}
     for fmt in (rb.LINKS_F64_18, rb.LINKS_F64_12, rb.LINKS_F32_18, rb.LINKS_F32_12):

@@ -13,6 +13,11 @@ sys.path.insert(0, ROOT)
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    # the C ABI library is the product under test: build it in-tree if it is missing
+    lib = os.path.join(ROOT, "rhmc-on-gpu_b200", "librhmc_b200.so")
+    if not os.path.exists(lib):
+        import subprocess
+        subprocess.check_call(["make", "-C", os.path.join(ROOT, "rhmc-on-gpu_b200"), "-j8"])
 
 
 def has_gpu():
