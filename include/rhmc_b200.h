@@ -229,6 +229,13 @@ int rhmc_last_inv_approx_calc(rhmc_ctx *ctx, double res);
 int rhmc_calc_ipdot(rhmc_ctx *ctx);
 int rhmc_calc_ipdot_gauge(rhmc_ctx *ctx);
 int rhmc_calc_ipdot_fermion(rhmc_ctx *ctx);
+/* The action whose link derivative rhmc_calc_ipdot_fermion is: S_f = sum over pseudofermions of
+ * chi^dag r_md(M^dag M) chi = a0 |chi|^2 + sum_i a_i Re<chi, (M^dag M + b_i)^-1 chi> with the
+ * rescaled md approximation and the md solver settings (the pole set fermionforce solves for,
+ * lib/Action/fermionforce.cc:27-38).  With U -> exp(i t Q) U on one link (Q hermitian),
+ * dS_f/dt = Re(i Tr(Q ipdot)) for the ipdot of rhmc_calc_ipdot_fermion: the action/force pair
+ * checked by finite differences. */
+int rhmc_fermion_action(rhmc_ctx *ctx, double *out);
 /* One MD trajectory with the configured integrator (update_nometro, update.cc:17-53). */
 int rhmc_update_nometro(rhmc_ctx *ctx);
 /* One RHMC trajectory (update, update.cc:58-152) from the momenta and phi set by the caller:

@@ -142,6 +142,34 @@ static int fermion_part(rhmc_ctx *c, int add)
     return fermion_force(c, d->P.no_ps, ap.order, ap.a.data(), xs, add);
 }
 
+// S_f = sum_ps chi_ps^dag r_md(M^dag M) chi_ps = sum_ps [a0 |chi|^2 + sum_i a_i Re<chi, x_i>]
+// with the rescaled md approximation: the action whose derivative calc_ipdot_fermion is
+// (the md pole set of fermionforce, lib/Action/fermionforce.cc:27-38)
+static int fermion_action_md(rhmc_ctx *c, double *out)
+{
+    int rc = check_ready(c);
+    if (rc) return rc;
+    Driver *d = drv(c);
+    const Approx ap = rescaled(c, 1);
+    double2 *chi, *xs;
+    if ((rc = field(c, "drv_chi", d->P.no_ps, &chi))) return rc;
+    if ((rc = field(c, "drv_x", (size_t)d->P.no_ps * ap.order, &xs))) return rc;
+    rc = solve(c, ap, d->P.residue_md, d->P.md_mode, d->P.md_fmt, chi, xs);
+    if (rc) return rc;
+    double s = 0.0, v;
+    for (int ps = 0; ps < d->P.no_ps; ps++) {
+        const double2 *cp = chi + ps * SP(c);
+        if ((rc = rdot(c, cp, cp, (long)SP(c), &v))) return rc;
+        s += ap.a0 * v;
+        for (int i = 0; i < ap.order; i++) {
+            if ((rc = rdot(c, cp, xs + ((size_t)ps * ap.order + i) * SP(c), (long)SP(c), &v))) return rc;
+            s += ap.a[i] * v;
+        }
+    }
+    *out = s;
+    return RHMC_OK;
+}
+
 static int calc_ipdot_full(rhmc_ctx *c)
 {
     int rc = gauge_force(c, 0);
@@ -408,6 +436,7 @@ int rhmc_calc_ipdot(rhmc_ctx *c) { return c ? calc_ipdot_full(c) : fail(RHMC_ERR
 int rhmc_calc_ipdot_gauge(rhmc_ctx *c) { return c ? gauge_force(c, 0) : fail(RHMC_ERR_ARG, "null"); }
 int rhmc_calc_ipdot_fermion(rhmc_ctx *c) { return c ? fermion_part(c, 0) : fail(RHMC_ERR_ARG, "null"); }
 int rhmc_update_nometro(rhmc_ctx *c) { return c ? update_nometro(c) : fail(RHMC_ERR_ARG, "null"); }
+int rhmc_fermion_action(rhmc_ctx *c, double *out) { return (c && out) ? fermion_action_md(c, out) : fail(RHMC_ERR_ARG, "null"); }
 int rhmc_save_conf(rhmc_ctx *c) { return c ? save_conf(c) : fail(RHMC_ERR_ARG, "null"); }
 int rhmc_copy_saved(rhmc_ctx *c) { return c ? copy_saved(c) : fail(RHMC_ERR_ARG, "null"); }
 

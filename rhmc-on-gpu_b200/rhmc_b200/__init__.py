@@ -404,3 +404,5 @@ class Legacy:
 
     def __getattr__(self, name):  # cuda_init0, cuda_init1, cuda_end, cuda_gauge_deriv, ...
         return getattr(self.L, name)
+
+Context.fermion_action = lambda self: _f(self, "rhmc_fermion_action")
