@@ -240,6 +240,221 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, nrhs=4, nshift=16, res=1e-
     return out
 
 
+NF_ML, NF_MS, NF_BETA, NF_DEG = 0.01, 0.05, 5.8, 15
+
+
+def _timed(torch, stream, fn, reps):
+    """Average device time (ms) of fn() issued reps times on stream, CUDA events on that stream."""
+    fn()
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+    stream.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
+    """N_f = 2+1 RHMC at 32^4 (light am=0.01 with N_f=2, strange am=0.05 with N_f=1, one
+    pseudofermion each, degree-15 rational approximations, beta=5.8, Haar hot start seed 1001,
+    momenta seed 3003, phi seeds 2002/2003, Metropolis uniform seed 4004; synthetic data).
+
+    1. MD kernels at this volume: device time and algorithmic bytes of the gauge force, the
+       fermion force (both species' 30 shifted solutions), the momentum and the link update.
+    2. The fermion force against central finite differences of S_f (md approximation, both
+       species) with eps = 1e-5 along fd_dirs random su(3) directions (seed 5005) on fd_links
+       random links (seed 6006).  At this volume S_f ~ 1e6, so S(+eps) - S(-eps) taken as the
+       difference of two separately summed actions loses ~11 digits; the central difference is
+       therefore also evaluated exactly as sum_i a_i Re<x_i(+), (A(-) - A(+)) x_i(-)> with
+       A = M^dag M + b_i and x_i(+-) the solutions at the two perturbed configurations (the
+       second resolvent identity, no approximation): A(-) - A(+) is non-zero only next to the
+       perturbed link, so nothing cancels.  Both are reported.
+    3. One leapfrog trajectory (tau = 1, 20 steps) with all-FP64 solves and with the mixed
+       solver for the force (FP64 heatbath/action solves): seconds per trajectory, Delta H,
+       acceptance and plaquette of both."""
+    from scipy.linalg import expm
+    from rhmc_b200 import rational as R
+    from rhmc_b200 import replicas as RP
+    # torch work (link edits, inner products) must be ordered with the library's launches
+    torch.cuda.set_stream(stream)
+    dims = DIMS
+    V = int(np.prod(dims))
+    Vh = V // 2
+    ctx = rb.Context(dims, mass=NF_ML, beta=NF_BETA, device=dev.index or 0)
+    ctx.set_stream(stream.cuda_stream)
+    u = F.random_links(dims, seed=RP.replica_seed(1001, rank))
+    u_traj = u if a.nf_start == "haar" else F.random_links(dims, seed=RP.replica_seed(1001, rank), kind="near1", eps=0.3)
+    ctx.set_gauge(u)
+    P0 = F.random_momenta(dims, seed=RP.replica_seed(3003, rank))
+    phis = [F.random_spinor(dims, seed=RP.replica_seed(2002, rank), n=1),
+            F.random_spinor(dims, seed=RP.replica_seed(2003, rank), n=1)]
+    uniform = float(np.random.Generator(np.random.Philox(RP.replica_seed(4004, rank))).random())
+    # spectral bounds: lambda_max by power iteration, lambda_min = m^2 (M^dag M = m^2 - D_eo D_oe >= m^2)
+    lmax = ctx.find_max(F.random_spinor(dims, seed=7007))
+    species = [(NF_ML, 2), (NF_MS, 1)]
+    bounds, approx = [], []
+    for m, nf in species:
+        lo, hi = m * m, lmax + m * m - NF_ML * NF_ML
+        eps = 0.95 * lo / (1.05 * hi)
+        bounds.append((lo, hi))
+        approx.append([R.rational_power(nf / 8.0, NF_DEG, eps), R.rational_power(-nf / 4.0, NF_DEG, eps),
+                       R.rational_power(-nf / 4.0, NF_DEG, eps)])
+    out = {"config": {"lattice": list(dims), "beta": NF_BETA, "species": [{"mass": m, "no_flavours": nf, "no_ps": 1}
+                                                                         for m, nf in species],
+                      "degree": NF_DEG, "eig_bounds": bounds, "start": "Haar (hot) for kernels and finite differences; "
+                      + ("Haar" if a.nf_start == "haar" else "exp(i 0.3 H) of a Gaussian algebra element H per link")
+                      + " for the trajectories",
+                      "approx_max_rel_err": max(c["max_rel_err"] for ap_ in approx for c in ap_)}}
+
+    def configure(md_mode, md_fmt, residue_md, no_md=20):
+        ctx.driver_setup(no_flavours=2, no_ps=1, no_md=no_md, integrator=rb.INT_LEAPFROG, residue_metro=1e-10,
+                         residue_md=residue_md, md_mode=md_mode, md_fmt=md_fmt)
+        if not getattr(ctx, "_nf_species", False):
+            ctx._nf_species = ctx.add_species(NF_MS, 1, 1)
+        for s in range(2):
+            ctx.select_species(s)
+            for w in range(3):
+                ctx.set_approx(w, approx[s][w])
+            ctx.set_eig_bounds(*bounds[s])
+            ctx.set_phi(phis[s])
+        ctx.select_species(0)
+
+    # ---- 1. MD kernels
+    configure(rb.MSOLVE_FP64, rb.LINKS_F64_18, 1e-10)
+    ctx.first_inv_approx_calc(1e-10)
+    ctx.set_momenta(P0)
+    nv = 2 * NF_DEG
+    xk = torch.randn(nv * 6 * Vh, dtype=torch.float64, device=dev)
+    coef = np.linspace(0.1, 1.0, nv)
+    reps = 5
+    kern = {}
+    kern["gauge_force"] = (_timed(torch, stream, lambda: ctx.gauge_force(0), reps), 4 * V * (144 + 64))
+    kern["fermion_force_30_vectors"] = (_timed(torch, stream, lambda: ctx.fermion_force(xk, coef, nrhs=1, add=1), reps),
+                                        4 * V * (144 + 128) + -(-nv // 8) * 4 * V * 144 + nv * (Vh * 96 + V * 48))
+    kern["mom_update"] = (_timed(torch, stream, lambda: ctx.mom_update(0.0), reps), 4 * V * 3 * 64)
+    kern["link_update"] = (_timed(torch, stream, lambda: ctx.link_update(0.0), reps), 4 * V * (64 + 2 * 144))
+    peak, _ = load_peaks()
+    out["kernels"] = {k: {"ms": round(t, 4), "alg_bytes": b, "gbs": round(b / (t * 1e-3) / 1e9, 1),
+                          "frac": round(b / (t * 1e-3) / 1e9 / peak, 4)} for k, (t, b) in kern.items()}
+    out["kernels"]["note"] = ("fermion_force = D_oe of the 30 vectors batched 8 per link read, then the outer-product/TA "
+                              "kernel; bytes: links + ipdot read-modify-write, links once per 8 vectors, per vector "
+                              "the spinor in/out of D_oe and the x and h reads of the force kernel")
+    del xk
+    ctx.set_gauge(u)
+
+    # ---- 2. finite differences of S_f
+    if a.fd_links > 0:
+        configure(rb.MSOLVE_FP64, rb.LINKS_F64_18, 1e-10)
+        ctx.first_inv_approx_calc(1e-10)
+        chis = []
+        for s in range(2):
+            ctx.select_species(s)
+            c_int = torch.zeros(6 * Vh, dtype=torch.float64, device=dev)
+            ctx.spinor_to_internal(rb.LINKS_F64_18, c_int, ctx.get_chi()[0])
+            chis.append(c_int)
+        ctx.select_species(0)
+        ctx.calc_ipdot_fermion()
+        ip = ctx.get_ipdot()
+        md = []
+        for s, (m, nf) in enumerate(species):
+            r = R.rescale(approx[s][1], 1.05 * bounds[s][1], -nf / 4.0)
+            md.append((np.array(r["b"]) + (m * m - NF_ML * NF_ML), np.array(r["a"]), r["a0"]))
+        rng = np.random.Generator(np.random.Philox(6006))
+        links = rng.choice(4 * V, size=a.fd_links, replace=False)
+        Qs = F.random_algebra(a.fd_dirs, np.random.Generator(np.random.Philox(5005)))
+        u_dev = torch.from_numpy(u).to(dev)
+        xs = {k: torch.zeros(NF_DEG * 6 * Vh, dtype=torch.float64, device=dev) for k in ("m0", "m1", "p0", "p1")}
+        w1 = [torch.zeros(NF_DEG * 6 * Vh, dtype=torch.float64, device=dev) for _ in range(2)]
+        w2 = torch.zeros(NF_DEG * 6 * Vh, dtype=torch.float64, device=dev)
+        h = 1e-5
+        errs, errs_plain, t_fd = [], [], time.perf_counter()
+        for l in links:
+            ul = u[l].copy()
+            for Q in Qs:
+                exact = float((1j * np.trace(Q @ ip[l])).real)
+                scale = float(np.linalg.norm(Q) * np.linalg.norm(ip[l]))
+                S = {}
+                for sign in (-1, 1):
+                    u_dev[l] = torch.from_numpy(expm(1j * sign * h * Q) @ ul).to(dev)
+                    ctx.set_gauge(u_dev)
+                    tag = "m" if sign < 0 else "p"
+                    for s in range(2):
+                        x = xs[tag + str(s)]
+                        ctx.msolve(x, chis[s], md[s][0], 1e-10, certify=1)
+                        xv = x.view(NF_DEG, 6 * Vh)
+                        S[(sign, s)] = md[s][2] * float(torch.dot(chis[s], chis[s])) + float(
+                            (torch.as_tensor(md[s][1], device=dev) * (xv @ chis[s])).sum())
+                        if sign < 0:
+                            ctx.mdagm(rb.LINKS_F64_18, w1[s], xs["m" + str(s)], 0.0, NF_DEG)
+                        else:
+                            ctx.mdagm(rb.LINKS_F64_18, w2, xs["m" + str(s)], 0.0, NF_DEG)
+                            d = (xs["p" + str(s)].view(NF_DEG, 6 * Vh) * (w1[s] - w2).view(NF_DEG, 6 * Vh)).sum(1)
+                            S[("id", s)] = float((torch.as_tensor(md[s][1], device=dev) * d).sum())
+                u_dev[l] = torch.from_numpy(ul).to(dev)
+                fd_id = (S[("id", 0)] + S[("id", 1)]) / (2 * h)
+                fd_plain = sum(S[(1, s)] - S[(-1, s)] for s in range(2)) / (2 * h)
+                errs.append(abs(fd_id - exact) / scale)
+                errs_plain.append(abs(fd_plain - exact) / scale)
+            print("fd: link %d done, %d pairs, max rel err %.3g, %.1f s" % (l, len(errs), max(errs), time.perf_counter() - t_fd),
+                  file=sys.stderr, flush=True)
+        ctx.set_gauge(u)
+        out["fd_check"] = {"pairs": len(errs), "links": int(a.fd_links), "directions": int(a.fd_dirs), "eps": h,
+                           "solve_true_residual": 1e-10,
+                           "max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs)),
+                           "max_rel_err_plain_difference": float(max(errs_plain)),
+                           "rel_err_definition": "|FD - Re i Tr(Q ipdot_l)| / (|Q| |ipdot_l|)",
+                           "target": 1e-8, "seconds": round(time.perf_counter() - t_fd, 1)}
+        del u_dev, xs, w1, w2
+
+    # ---- 3. trajectories: the MD evolution alone (plaquette of the proposal), then the full update
+    traj = {}
+    bounds_traj = bounds
+    if a.nf_start != "haar":
+        ctx.set_gauge(u_traj)
+        lmax_t = ctx.find_max(F.random_spinor(dims, seed=7007))
+        bounds_traj = [(m * m, lmax_t + m * m - NF_ML * NF_ML) for m, _ in species]
+        if lmax_t > lmax:
+            raise RuntimeError("trajectory start has a larger spectral radius than the approximations cover")
+    for name, mode, fmt in (("fp64", rb.MSOLVE_FP64, rb.LINKS_F64_18), ("mixed", rb.MSOLVE_MIXED, rb.LINKS_F64_12)):
+        configure(mode, fmt, 1e-8, no_md=a.nf_steps)
+        for s in range(2):
+            ctx.select_species(s)
+            ctx.set_eig_bounds(*bounds_traj[s])
+        ctx.select_species(0)
+        ctx.set_gauge(u_traj)
+        ctx.set_momenta(P0)
+        ctx.first_inv_approx_calc(1e-10)
+        stream.synchronize()
+        t0 = time.perf_counter()
+        ctx.update_nometro()
+        stream.synchronize()
+        t_md = time.perf_counter() - t0
+        plaq_md = ctx.plaquette()
+        ctx.set_gauge(u_traj)
+        ctx.set_momenta(P0)
+        stream.synchronize()
+        n0 = ctx.launch_count()
+        t0 = time.perf_counter()
+        dS, acc = ctx.update(uniform)
+        stream.synchronize()
+        dt = time.perf_counter() - t0
+        traj[name] = {"s_per_trajectory": round(dt, 3), "s_md_only": round(t_md, 3), "delta_H": dS, "accepted": acc,
+                      "plaquette_proposal": plaq_md, "plaquette_after": ctx.plaquette(),
+                      "gpu_launches": ctx.launch_count() - n0}
+    traj["speedup_mixed_vs_fp64"] = round(traj["fp64"]["s_per_trajectory"] / traj["mixed"]["s_per_trajectory"], 3)
+    traj["delta_H_abs_diff"] = abs(traj["fp64"]["delta_H"] - traj["mixed"]["delta_H"])
+    traj["integrator"] = "leapfrog tau=1, %d steps; md residual 1e-8, metro residual 1e-10 (FP64)" % a.nf_steps
+    traj["plaquette_proposal_abs_diff"] = max(abs(p - q) for p, q in zip(traj["fp64"]["plaquette_proposal"],
+                                                                           traj["mixed"]["plaquette_proposal"]))
+    out["trajectory"] = traj
+    ctx.close()
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -249,6 +464,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dims", default="32,32,32,32")
     ap.add_argument("--no-msolve", action="store_true")
+    ap.add_argument("--workload", default="dslash", choices=["dslash", "nf2p1"],
+                    help="dslash: the headline line (Dslash + multi-shift CG); nf2p1: N_f=2+1 forces, "
+                         "finite-difference check and trajectories")
+    ap.add_argument("--fd-links", type=int, default=16)
+    ap.add_argument("--fd-dirs", type=int, default=8)
+    ap.add_argument("--nf-steps", type=int, default=20)
+    ap.add_argument("--nf-start", default="near1", choices=["haar", "near1"])
     a = ap.parse_args()
     a.warmup = max(3, a.warmup)
     if a.impl == "reference":
@@ -273,6 +495,16 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+
+    if a.workload == "nf2p1":
+        stream = torch.cuda.Stream(device=dev)
+        res = nf2p1_bench(a, rb, F, np, torch, rank, dev, stream)
+        if rank == 0:
+            print(json.dumps({"workload": "nf2p1", "n_gpus": world, "data": "synthetic", **res}))
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     V = int(np.prod(DIMS))
     Vh = V // 2

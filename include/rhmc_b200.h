@@ -208,13 +208,23 @@ typedef struct {
     int md_mode, md_fmt;       /* ... of the force solves */
 } rhmc_driver_params;
 
-/* Configures the driver of lib/Update (update.cc, ipdot.cc, momenta.cc, MD_integrators). */
+/* Configures the driver of lib/Update (update.cc, ipdot.cc, momenta.cc, MD_integrators).
+ * no_flavours and no_ps describe species 0, the fermions at the context mass. */
 int rhmc_driver_setup(rhmc_ctx *ctx, const rhmc_driver_params *p);
+/* No counterpart in the reference (one species only): adds a fermion species of its own mass
+ * (>= the context mass), no_flavours and no_ps, e.g. the strange quark of N_f = 2+1, and returns
+ * its index (1, 2, ...).  It gets its own pseudofermions, rational approximations and eigenvalue
+ * bounds; heatbath, actions and forces then sum over all species.  Its solves run on the
+ * context's M^dag M with every pole shifted by mass^2 - context mass^2. */
+int rhmc_driver_add_species(rhmc_ctx *ctx, double mass, int no_flavours, int no_ps, int *index);
+/* Selects the species that rhmc_set_approx, rhmc_set_eig_bounds and rhmc_set/get_phi/chi act on
+ * (0 after setup). */
+int rhmc_driver_select_species(rhmc_ctx *ctx, int index);
 /* Normalised rational approximation on [min_eps, 1] (RationalApprox, rationalapprox.h:13-47):
  * which = 0 first (heatbath, x^(N_f/(8 N_ps))), 1 md (force), 2 last (action) (x^(-N_f/(4 N_ps))).
  * The coefficients rationalapprox_calc (rationalapprox_calc.cc:8-177) would compute at start-up. */
 int rhmc_set_approx(rhmc_ctx *ctx, int which, int order, double a0, const double *a, const double *b, double min_eps);
-/* Spectral bounds of M^dag M that findminmax would return (findminmax.cc:140-183); the rescaling
+/* Spectral bounds of M^dag M (at the selected species' mass) that findminmax would return (findminmax.cc:140-183); the rescaling
  * widens them by 0.95 / 1.05 like RationalApprox::*_inv_approx_coeff (rationalapprox.cc:134-266). */
 int rhmc_set_eig_bounds(rhmc_ctx *ctx, double min, double max);
 /* Pseudofermions phi and chi, reference layout complex[no_ps][Vh][3] (MultiFermion). */

@@ -16,8 +16,16 @@
 // The eigenvalue bounds that findminmax would compute (findminmax.cc:140-183) are supplied by
 // the caller (rhmc_set_eig_bounds); they are widened by 0.95/1.05 as the reference does.
 // Fields stay on the device for the whole trajectory; nothing is reallocated per trajectory.
+//
+// Fermion species.  The reference has one species (mass, no_flavours, no_ps).  Further species
+// (e.g. the strange quark of N_f = 2+1) are added with rhmc_driver_add_species; each has its own
+// pseudofermions, rational approximations and eigenvalue bounds, and every heatbath, action and
+// force sums over all species.  A species of mass m_s >= the context mass m runs on the same
+// links and solver with every pole shifted by m_s^2 - m^2, since M^dag M(m_s) = M^dag M(m) +
+// m_s^2 - m^2 on the even sites.
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "capi_util.h"
@@ -42,22 +50,44 @@ struct Approx {
     std::vector<double> a, b;
 };
 
+struct Species {
+    double mass = 0;
+    int no_flavours = 0, no_ps = 0;
+    Approx approx[3];  // first (heatbath), md (force), last (action); normalised on [min_eps, 1]
+    double eig_min = 0, eig_max = 0;  // of M^dag M at this species' mass
+    bool have_bounds = false;
+};
+
 struct Driver {
     rhmc_driver_params P;
     bool configured = false;
-    Approx approx[3];  // first (heatbath), md (force), last (action); normalised on [min_eps, 1]
-    double eig_min = 0, eig_max = 0;
-    bool have_bounds = false;
+    std::vector<Species> sp;  // sp[0]: the context mass with P.no_flavours, P.no_ps
+    int cur = 0;              // the species the approx / bounds / phi / chi setters act on
     long force_evals = 0, solves = 0;
 };
 
 static Driver *drv(rhmc_ctx *c) { return c->driver; }
 
+static Driver *ensure_driver(rhmc_ctx *c)
+{
+    if (!c->driver) {
+        c->driver = new Driver();
+        c->driver->sp.resize(1);
+        c->driver->sp[0].mass = c->mass;
+    }
+    return c->driver;
+}
+
+static int nspecies(rhmc_ctx *c) { return (int)drv(c)->sp.size(); }
+
+// workspace name of a per-species field: "drv_phi", "drv_phi.1", ...
+static std::string fname(const char *base, int s) { return s == 0 ? std::string(base) : std::string(base) + "." + std::to_string(s); }
+
 void driver_free(Driver *d) { delete d; }
 
 static size_t SP(rhmc_ctx *c) { return 3 * (size_t)c->Vh; }
 
-static int field(rhmc_ctx *c, const char *name, size_t n_spinors, double2 **out)
+static int field(rhmc_ctx *c, const std::string &name, size_t n_spinors, double2 **out)
 {
     void *p;
     CK(c->ws.get(name, n_spinors * SP(c) * sizeof(double2), &p));
@@ -65,14 +95,14 @@ static int field(rhmc_ctx *c, const char *name, size_t n_spinors, double2 **out)
     return RHMC_OK;
 }
 
-// RationalApprox::*_inv_approx_coeff (rationalapprox.cc:134-266)
-static Approx rescaled(rhmc_ctx *c, int which)
+// RationalApprox::*_inv_approx_coeff (rationalapprox.cc:134-266) for species s
+static Approx rescaled(rhmc_ctx *c, int s, int which)
 {
-    Driver *d = drv(c);
-    Approx r = d->approx[which];
-    const double mx = d->eig_max * 1.05;
-    const double ex = which == 0 ? ((double)d->P.no_flavours) / 8. / ((double)d->P.no_ps)
-                                 : -((double)d->P.no_flavours) / 4. / ((double)d->P.no_ps);
+    const Species &S = drv(c)->sp[s];
+    Approx r = S.approx[which];
+    const double mx = S.eig_max * 1.05;
+    const double ex = which == 0 ? ((double)S.no_flavours) / 8. / ((double)S.no_ps)
+                                 : -((double)S.no_flavours) / 4. / ((double)S.no_ps);
     const double e = pow(mx, ex);
     r.a0 *= e;
     for (int i = 0; i < r.order; i++) {
@@ -82,14 +112,19 @@ static Approx rescaled(rhmc_ctx *c, int which)
     return r;
 }
 
-static int solve(rhmc_ctx *c, const Approx &ap, double res, int mode, int fmt, const double2 *b, double2 *x)
+// (M^dag M(m_s) + b_i) x_i = b for the species' pseudofermions, on the context's M^dag M(m)
+static int solve(rhmc_ctx *c, int s, const Approx &ap, double res, int mode, int fmt, const double2 *b, double2 *x)
 {
     Driver *d = drv(c);
+    const double dm2 = d->sp[s].mass * d->sp[s].mass - c->mass * c->mass;
+    std::vector<double> shifts(ap.b);
+    if (s != 0)
+        for (double &v : shifts) v += dm2;
     rhmc_msolve_params mp;
     memset(&mp, 0, sizeof(mp));
     mp.nshift = ap.order;
-    mp.shifts = ap.b.data();
-    mp.nrhs = d->P.no_ps;
+    mp.shifts = shifts.data();
+    mp.nrhs = d->sp[s].no_ps;
     mp.residual = res;
     mp.max_iter = d->P.max_cg;
     mp.mode = mode;
@@ -102,44 +137,60 @@ static int check_ready(rhmc_ctx *c)
 {
     Driver *d = drv(c);
     if (!d || !d->configured) return fail(RHMC_ERR_STATE, "driver not configured (rhmc_driver_setup)");
-    if (!d->have_bounds) return fail(RHMC_ERR_STATE, "eigenvalue bounds not set (rhmc_set_eig_bounds)");
-    for (int w = 0; w < 3; w++)
-        if (d->approx[w].order < 1) return fail(RHMC_ERR_STATE, "rational approximation %d not set (rhmc_set_approx)", w);
+    for (int s = 0; s < nspecies(c); s++) {
+        const Species &S = d->sp[s];
+        if (!S.have_bounds) return fail(RHMC_ERR_STATE, "species %d: eigenvalue bounds not set (rhmc_set_eig_bounds)", s);
+        for (int w = 0; w < 3; w++)
+            if (S.approx[w].order < 1)
+                return fail(RHMC_ERR_STATE, "species %d: rational approximation %d not set (rhmc_set_approx)", s, w);
+    }
     return RHMC_OK;
 }
 
-// chi = r_first(M^dag M) phi (first_inv_approx_calc) or phi = r_last(M^dag M) chi (last_...)
+// chi = r_first(M^dag M) phi (first_inv_approx_calc) or phi = r_last(M^dag M) chi (last_...),
+// for every species
 static int inv_approx_calc(rhmc_ctx *c, int which, double res)
 {
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
-    const Approx ap = rescaled(c, which);
-    double2 *phi, *chi, *xs;
-    if ((rc = field(c, "drv_phi", d->P.no_ps, &phi))) return rc;
-    if ((rc = field(c, "drv_chi", d->P.no_ps, &chi))) return rc;
-    if ((rc = field(c, "drv_x", (size_t)d->P.no_ps * ap.order, &xs))) return rc;
-    const double2 *in = which == 0 ? phi : chi;
-    double2 *out = which == 0 ? chi : phi;
-    rc = solve(c, ap, res, d->P.metro_mode, d->P.metro_fmt, in, xs);
-    if (rc) return rc;
-    return rational_sum(c, d->P.no_ps, ap.order, ap.a0, ap.a.data(), xs, in, out);
+    for (int s = 0; s < nspecies(c); s++) {
+        const int nps = d->sp[s].no_ps;
+        const Approx ap = rescaled(c, s, which);
+        double2 *phi = nullptr, *chi = nullptr, *xs = nullptr;
+        rc = field(c, fname("drv_phi", s), nps, &phi);
+        if (rc) return rc;
+        rc = field(c, fname("drv_chi", s), nps, &chi);
+        if (rc) return rc;
+        rc = field(c, "drv_x", (size_t)nps * ap.order, &xs);
+        if (rc) return rc;
+        const double2 *in = which == 0 ? phi : chi;
+        double2 *out = which == 0 ? chi : phi;
+        if ((rc = solve(c, s, ap, res, d->P.metro_mode, d->P.metro_fmt, in, xs))) return rc;
+        if ((rc = rational_sum(c, nps, ap.order, ap.a0, ap.a.data(), xs, in, out))) return rc;
+    }
+    return RHMC_OK;
 }
 
-// calc_ipdot_fermion (overwrite) or its part of calc_ipdot (add)
+// calc_ipdot_fermion (overwrite) or its part of calc_ipdot (add): the sum over species
 static int fermion_part(rhmc_ctx *c, int add)
 {
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
-    const Approx ap = rescaled(c, 1);
-    double2 *chi, *xs;
-    if ((rc = field(c, "drv_chi", d->P.no_ps, &chi))) return rc;
-    if ((rc = field(c, "drv_x", (size_t)d->P.no_ps * ap.order, &xs))) return rc;
-    rc = solve(c, ap, d->P.residue_md, d->P.md_mode, d->P.md_fmt, chi, xs);
-    if (rc) return rc;
+    for (int s = 0; s < nspecies(c); s++) {
+        const int nps = d->sp[s].no_ps;
+        const Approx ap = rescaled(c, s, 1);
+        double2 *chi = nullptr, *xs = nullptr;
+        rc = field(c, fname("drv_chi", s), nps, &chi);
+        if (rc) return rc;
+        rc = field(c, "drv_x", (size_t)nps * ap.order, &xs);
+        if (rc) return rc;
+        if ((rc = solve(c, s, ap, d->P.residue_md, d->P.md_mode, d->P.md_fmt, chi, xs))) return rc;
+        if ((rc = fermion_force(c, nps, ap.order, ap.a.data(), xs, s == 0 ? add : 1))) return rc;
+    }
     d->force_evals++;
-    return fermion_force(c, d->P.no_ps, ap.order, ap.a.data(), xs, add);
+    return RHMC_OK;
 }
 
 // S_f = sum_ps chi_ps^dag r_md(M^dag M) chi_ps = sum_ps [a0 |chi|^2 + sum_i a_i Re<chi, x_i>]
@@ -150,23 +201,27 @@ static int fermion_action_md(rhmc_ctx *c, double *out)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
-    const Approx ap = rescaled(c, 1);
-    double2 *chi, *xs;
-    if ((rc = field(c, "drv_chi", d->P.no_ps, &chi))) return rc;
-    if ((rc = field(c, "drv_x", (size_t)d->P.no_ps * ap.order, &xs))) return rc;
-    rc = solve(c, ap, d->P.residue_md, d->P.md_mode, d->P.md_fmt, chi, xs);
-    if (rc) return rc;
-    double s = 0.0, v;
-    for (int ps = 0; ps < d->P.no_ps; ps++) {
-        const double2 *cp = chi + ps * SP(c);
-        if ((rc = rdot(c, cp, cp, (long)SP(c), &v))) return rc;
-        s += ap.a0 * v;
-        for (int i = 0; i < ap.order; i++) {
-            if ((rc = rdot(c, cp, xs + ((size_t)ps * ap.order + i) * SP(c), (long)SP(c), &v))) return rc;
-            s += ap.a[i] * v;
+    double sum = 0.0, v;
+    for (int s = 0; s < nspecies(c); s++) {
+        const int nps = d->sp[s].no_ps;
+        const Approx ap = rescaled(c, s, 1);
+        double2 *chi = nullptr, *xs = nullptr;
+        rc = field(c, fname("drv_chi", s), nps, &chi);
+        if (rc) return rc;
+        rc = field(c, "drv_x", (size_t)nps * ap.order, &xs);
+        if (rc) return rc;
+        if ((rc = solve(c, s, ap, d->P.residue_md, d->P.md_mode, d->P.md_fmt, chi, xs))) return rc;
+        for (int ps = 0; ps < nps; ps++) {
+            const double2 *cp = chi + ps * SP(c);
+            if ((rc = rdot(c, cp, cp, (long)SP(c), &v))) return rc;
+            sum += ap.a0 * v;
+            for (int i = 0; i < ap.order; i++) {
+                if ((rc = rdot(c, cp, xs + ((size_t)ps * ap.order + i) * SP(c), (long)SP(c), &v))) return rc;
+                sum += ap.a[i] * v;
+            }
         }
     }
-    *out = s;
+    *out = sum;
     return RHMC_OK;
 }
 
@@ -344,11 +399,18 @@ static int action(rhmc_ctx *c, int final_part, double *out)
     int rc = plaquette_sums(c, &t, &sp);
     if (rc) return rc;
     if ((rc = momentum_action(c, &m))) return rc;
-    double2 *phi, *chi;
-    if ((rc = field(c, "drv_phi", d->P.no_ps, &phi))) return rc;
-    if ((rc = field(c, "drv_chi", d->P.no_ps, &chi))) return rc;
-    // initial: sum Re<phi, phi>; final: sum Re<phi, chi> with phi = r_last chi
-    if ((rc = rdot(c, phi, final_part ? chi : phi, (long)d->P.no_ps * SP(c), &f))) return rc;
+    // initial: sum Re<phi, phi>; final: sum Re<phi, chi> with phi = r_last chi; over all species
+    for (int s = 0; s < nspecies(c); s++) {
+        const int nps = d->sp[s].no_ps;
+        double2 *phi = nullptr, *chi = nullptr;
+        double fs;
+        rc = field(c, fname("drv_phi", s), nps, &phi);
+        if (rc) return rc;
+        rc = field(c, fname("drv_chi", s), nps, &chi);
+        if (rc) return rc;
+        if ((rc = rdot(c, phi, final_part ? chi : phi, (long)nps * SP(c), &fs))) return rc;
+        f += fs;
+    }
     *out = (c->beta / 3.0) * (t + sp) + m + f;
     return RHMC_OK;
 }
@@ -384,17 +446,44 @@ int rhmc_driver_setup(rhmc_ctx *c, const rhmc_driver_params *p)
     if (p->no_ps < 1 || p->no_flavours < 1 || p->no_md < 1 || p->gauge_scale < 1 || p->max_cg < 1)
         return fail(RHMC_ERR_ARG, "no_ps, no_flavours, no_md, gauge_scale and max_cg must be positive");
     if (p->integrator < 0 || p->integrator > RHMC_INT_LEAPFROG) return fail(RHMC_ERR_ARG, "unknown integrator");
-    if (!c->driver) c->driver = new Driver();
-    c->driver->P = *p;
-    c->driver->configured = true;
+    Driver *d = ensure_driver(c);
+    d->P = *p;
+    d->sp[0].no_flavours = p->no_flavours;
+    d->sp[0].no_ps = p->no_ps;
+    d->configured = true;
+    return RHMC_OK;
+}
+
+int rhmc_driver_add_species(rhmc_ctx *c, double mass, int no_flavours, int no_ps, int *index)
+{
+    if (!c || !index) return fail(RHMC_ERR_ARG, "null argument");
+    if (!(mass >= c->mass)) return fail(RHMC_ERR_ARG, "species mass %g below the context mass %g", mass, c->mass);
+    if (no_flavours < 1 || no_ps < 1) return fail(RHMC_ERR_ARG, "no_flavours and no_ps must be positive");
+    Driver *d = ensure_driver(c);
+    if (d->sp.size() >= 8) return fail(RHMC_ERR_ARG, "at most 8 species");
+    Species S;
+    S.mass = mass;
+    S.no_flavours = no_flavours;
+    S.no_ps = no_ps;
+    d->sp.push_back(S);
+    *index = (int)d->sp.size() - 1;
+    return RHMC_OK;
+}
+
+int rhmc_driver_select_species(rhmc_ctx *c, int index)
+{
+    if (!c) return fail(RHMC_ERR_ARG, "null argument");
+    Driver *d = ensure_driver(c);
+    if (index < 0 || index >= (int)d->sp.size()) return fail(RHMC_ERR_ARG, "no species %d", index);
+    d->cur = index;
     return RHMC_OK;
 }
 
 int rhmc_set_approx(rhmc_ctx *c, int which, int order, double a0, const double *a, const double *b, double min_eps)
 {
     if (!c || !a || !b || which < 0 || which > 2 || order < 1 || order > 32) return fail(RHMC_ERR_ARG, "bad argument");
-    if (!c->driver) c->driver = new Driver();
-    Approx &ap = c->driver->approx[which];
+    Driver *d = ensure_driver(c);
+    Approx &ap = d->sp[d->cur].approx[which];
     ap.order = order;
     ap.a0 = a0;
     ap.min_eps = min_eps;
@@ -406,20 +495,23 @@ int rhmc_set_approx(rhmc_ctx *c, int which, int order, double a0, const double *
 int rhmc_set_eig_bounds(rhmc_ctx *c, double min, double max)
 {
     if (!c || !(max > 0.0) || !(min > 0.0) || min > max) return fail(RHMC_ERR_ARG, "need 0 < min <= max");
-    if (!c->driver) c->driver = new Driver();
-    c->driver->eig_min = min;
-    c->driver->eig_max = max;
-    c->driver->have_bounds = true;
+    Driver *d = ensure_driver(c);
+    Species &S = d->sp[d->cur];
+    S.eig_min = min;
+    S.eig_max = max;
+    S.have_bounds = true;
     return RHMC_OK;
 }
 
+// the pseudofermions of the selected species
 static int pf_io(rhmc_ctx *c, const char *name, double *host_ref, int location, int to_device)
 {
     if (!c || !host_ref) return fail(RHMC_ERR_ARG, "null argument");
     if (!c->driver || !c->driver->configured) return fail(RHMC_ERR_STATE, "driver not configured");
-    const int n = c->driver->P.no_ps;
+    const int s = c->driver->cur;
+    const int n = c->driver->sp[s].no_ps;
     double2 *f;
-    int rc = field(c, name, n, &f);
+    int rc = field(c, fname(name, s), n, &f);
     if (rc) return rc;
     if (to_device) return rhmc_spinor_to_internal(c, RHMC_LINKS_F64_18, f, host_ref, n, location);
     return rhmc_spinor_from_internal(c, RHMC_LINKS_F64_18, host_ref, f, n, location);

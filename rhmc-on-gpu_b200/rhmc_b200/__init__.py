@@ -306,7 +306,9 @@ def _set_approx(self, which, approx):
 
 
 def _pf_get(self, name):
-    out = np.zeros((self.no_ps, self.Vh, 3), np.complex128)
+    cur = getattr(self, "_cur_species", 0)
+    nps = self.no_ps if cur == 0 else self._species_nps[cur]
+    out = np.zeros((nps, self.Vh, 3), np.complex128)
     self.call(name, out, HOST)
     return out
 
@@ -406,3 +408,38 @@ class Legacy:
         return getattr(self.L, name)
 
 Context.fermion_action = lambda self: _f(self, "rhmc_fermion_action")
+
+
+def _add_species(self, mass, no_flavours, no_ps):
+    """Adds a fermion species (rhmc_driver_add_species) and returns its index."""
+    idx = ctypes.c_int()
+    self.call("rhmc_driver_add_species", float(mass), int(no_flavours), int(no_ps), ctypes.byref(idx))
+    self._species_nps = getattr(self, "_species_nps", {})
+    self._species_nps[idx.value] = no_ps
+    return idx.value
+
+
+def _select_species(self, index):
+    self.call("rhmc_driver_select_species", int(index))
+    self._cur_species = int(index)
+
+
+Context.add_species = _add_species
+Context.select_species = _select_species
+
+
+def _find_max(self, start):
+    """Largest eigenvalue of M^dag M by FP64 power iteration (rhmc_find_max); start: host spinor."""
+    v = ctypes.c_double()
+    self.call("rhmc_find_max", np.ascontiguousarray(start, np.complex128), ctypes.byref(v))
+    return v.value
+
+
+def _find_min(self, start, mx):
+    v = ctypes.c_double()
+    self.call("rhmc_find_min", np.ascontiguousarray(start, np.complex128), float(mx), ctypes.byref(v))
+    return v.value
+
+
+Context.find_max = _find_max
+Context.find_min = _find_min

@@ -21,17 +21,25 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def _setup():
+def _setup(two_species=False):
     from gpu_util import new_ctx
     g = dict(np.load(os.path.join(HERE, "golden", "ref_t4.npz")))
     with open(os.path.join(HERE, "golden", "rational_coeffs.json")) as f:
         cf = json.load(f)["t4"]
-    ctx = new_ctx(tuple(g["dims"]), mass=float(g["mass"]), beta=float(g["beta"]))
+    m = float(g["mass"])
+    ctx = new_ctx(tuple(g["dims"]), mass=m, beta=float(g["beta"]))
     ctx.driver_setup(no_flavours=2, no_ps=1, residue_md=1e-13, residue_metro=1e-13)
     for w, c in enumerate(cf):
         ctx.set_approx(w, c)
     ctx.set_eig_bounds(*g["bounds"])
     ctx.set_chi(g["chi"])
+    if two_species:  # a heavier species (mass 0.25, one flavour) with its own pseudofermion
+        s = ctx.add_species(0.25, 1, 1)
+        ctx.select_species(s)
+        for w, c in enumerate(cf):
+            ctx.set_approx(w, c)
+        ctx.set_eig_bounds(*(np.array(g["bounds"]) + 0.25 ** 2 - m ** 2))
+        ctx.set_chi(F.random_spinor(tuple(g["dims"]), seed=2003, n=1))
     return ctx, g
 
 
@@ -46,15 +54,15 @@ def _fd(ctx, u, l, Q, action, h, four_point):
     return (S(h) - S(-h)) / (2 * h)
 
 
-@pytest.mark.parametrize("part", ["fermion", "gauge"])
+@pytest.mark.parametrize("part", ["fermion", "fermion_2species", "gauge"])
 def test_force_is_the_derivative_of_its_action(part):
-    ctx, g = _setup()
+    ctx, g = _setup(part == "fermion_2species")
     u = g["u"]
     rng = np.random.Generator(np.random.Philox(6006))
     links = rng.choice(u.shape[0], size=4, replace=False)
     Qs = F.random_algebra(4, np.random.Generator(np.random.Philox(5005)))
     ctx.set_gauge(u)
-    if part == "fermion":
+    if part.startswith("fermion"):
         ctx.calc_ipdot_fermion()
         action = ctx.fermion_action
     else:
