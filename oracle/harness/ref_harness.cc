@@ -158,6 +158,23 @@ void smartunpack_thmatrix(Momenta *out, float in[8 * no_links])
     }
 }
 
+// The reference packer itself (lib/Tools/Packer/packer.cc), compiled unmodified with its
+// functions renamed refpk_* (oracle/build_ref.py), for pinning the packed host formats.
+void refpk_smartpack_gauge(float out[2 * 12 * no_links], const Conf *in);
+void refpk_smartunpack_gauge(Conf *out, const float in[2 * 12 * no_links]);
+void refpk_smartpack_fermion(float out[6 * sizeh], const Fermion *in);
+void refpk_smartpack_fermion_d(float out[6 * sizeh * 2], const Fermion *in);
+void refpk_smartunpack_fermion_d(Fermion *out, const float in[6 * sizeh * 2]);
+void refpk_smartpack_multifermion(float out[6 * sizeh * no_ps * 2], const MultiFermion *in);
+void refpk_smartunpack_multifermion(MultiFermion *out, const float in[6 * sizeh * no_ps * 2]);
+void refpk_smartunpack_multishiftfermion(ShiftMultiFermion *out, const float in[6 * sizeh * max_approx_order * no_ps * 2],
+                                         int order);
+void refpk_make_shift_table(int table[8 * size]);
+void refpk_smartpack_tamatrix(float out[8 * no_links], Ipdot *in);
+void refpk_smartunpack_tamatrix(Ipdot *out, float in[8 * no_links]);
+void refpk_smartpack_thmatrix(float out[8 * no_links], Momenta *in);
+void refpk_smartunpack_thmatrix(Momenta *out, float in[8 * no_links]);
+
 // ------------------------------------------------------------------ extern "C" surface
 static Fermion *h_in = 0, *h_out = 0;
 
@@ -225,6 +242,33 @@ void ref_tables(int *table, int *eta_out)
         }
     for (long i = 0; i < no_links; i++) eta_out[i] = eta[i];
 }
+
+// packer I/O: the reference packer between the harness's exact fields and packed floats
+void ref_pk_gauge(float *out) { refpk_smartpack_gauge(out, gauge_conf); }
+void ref_unpk_gauge(const float *in) { refpk_smartunpack_gauge(gauge_conf, in); }
+void ref_pk_chi(float *out) { refpk_smartpack_multifermion(out, fermion_chi); }
+void ref_unpk_chi(const float *in) { refpk_smartunpack_multifermion(fermion_chi, in); }
+void ref_pk_fermion(float *out, const double *in)
+{
+    smartunpack_fermion_d(h_in, reinterpret_cast<const float *>(in));
+    refpk_smartpack_fermion(out, h_in);
+}
+void ref_pk_fermion_d(float *out, const double *in)
+{
+    smartunpack_fermion_d(h_in, reinterpret_cast<const float *>(in));
+    refpk_smartpack_fermion_d(out, h_in);
+}
+void ref_unpk_fermion_d(double *out, const float *in)
+{
+    refpk_smartunpack_fermion_d(h_in, in);
+    smartpack_fermion_d(reinterpret_cast<float *>(out), h_in);
+}
+void ref_unpk_shifted(const float *in, int order) { refpk_smartunpack_multishiftfermion(fermion_shiftmulti, in, order); }
+void ref_pk_ipdot(float *out) { refpk_smartpack_tamatrix(out, gauge_ipdot); }
+void ref_unpk_ipdot(const float *in) { refpk_smartunpack_tamatrix(gauge_ipdot, const_cast<float *>(in)); }
+void ref_pk_momenta(float *out) { refpk_smartpack_thmatrix(out, gauge_momenta); }
+void ref_unpk_momenta(const float *in) { refpk_smartunpack_thmatrix(gauge_momenta, const_cast<float *>(in)); }
+void ref_shift_table(int *table) { refpk_make_shift_table(table); }
 
 void ref_set_links(const double *u) { smartunpack_gauge(gauge_conf, reinterpret_cast<const float *>(u)); gauge_conf->save(); }
 void ref_get_links(double *u) { smartpack_gauge(reinterpret_cast<float *>(u), gauge_conf); }

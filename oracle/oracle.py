@@ -24,6 +24,11 @@ def _dp(a):
     return a.ctypes.data_as(_D)
 
 
+def _fp(a):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
 def _ip(a):
     assert a.flags.c_contiguous and a.dtype == np.int32
     return a.ctypes.data_as(_I)
@@ -78,6 +83,70 @@ class Oracle:
 
     def _reinit(self):
         self.lib.orc_init(*self.dims, self.bc)
+
+    # the reference packer (lib/Tools/Packer/packer.cc), between exact fields and packed floats
+    def _f32(self, n):
+        return np.zeros(n, np.float32)
+
+    def pk_gauge(self):
+        out = self._f32(2 * 12 * 4 * self.V)
+        self.lib.ref_pk_gauge(_fp(out))
+        return out
+
+    def unpk_gauge(self, pk):
+        self.lib.ref_unpk_gauge(_fp(np.ascontiguousarray(pk, np.float32)))
+        return self.get_links()
+
+    def pk_chi(self):
+        out = self._f32(6 * self.Vh * self.no_ps * 2)
+        self.lib.ref_pk_chi(_fp(out))
+        return out
+
+    def unpk_chi(self, pk):
+        self.lib.ref_unpk_chi(_fp(np.ascontiguousarray(pk, np.float32)))
+        return self.get_chi()
+
+    def pk_fermion(self, x):
+        out = self._f32(6 * self.Vh)
+        self.lib.ref_pk_fermion(_fp(out), _dp(np.ascontiguousarray(x, np.complex128)))
+        return out
+
+    def pk_fermion_d(self, x):
+        out = self._f32(6 * self.Vh * 2)
+        self.lib.ref_pk_fermion_d(_fp(out), _dp(np.ascontiguousarray(x, np.complex128)))
+        return out
+
+    def unpk_fermion_d(self, pk):
+        out = np.zeros((self.Vh, 3), np.complex128)
+        self.lib.ref_unpk_fermion_d(_dp(out), _fp(np.ascontiguousarray(pk, np.float32)))
+        return out
+
+    def unpk_shifted(self, pk, order):
+        self.lib.ref_unpk_shifted(_fp(np.ascontiguousarray(pk, np.float32)), order)
+        return self.get_shifted(order)
+
+    def pk_ipdot(self):
+        out = self._f32(8 * 4 * self.V)
+        self.lib.ref_pk_ipdot(_fp(out))
+        return out
+
+    def unpk_ipdot(self, pk):
+        self.lib.ref_unpk_ipdot(_fp(np.ascontiguousarray(pk, np.float32)))
+        return self.get_ipdot()
+
+    def pk_momenta(self):
+        out = self._f32(8 * 4 * self.V)
+        self.lib.ref_pk_momenta(_fp(out))
+        return out
+
+    def unpk_momenta(self, pk):
+        self.lib.ref_unpk_momenta(_fp(np.ascontiguousarray(pk, np.float32)))
+        return self.get_momenta()
+
+    def shift_table(self):
+        t = np.zeros(8 * self.V, np.int32)
+        self.lib.ref_shift_table(_ip(t))
+        return t
 
     def tables(self):
         t = np.zeros(8 * self.V, np.int32)
@@ -251,6 +320,70 @@ class RefLib:
         f = np.zeros((self.no_ps, order, self.Vh, 3), np.complex128)
         self.lib.ref_get_shifted(_dp(f), order)
         return f
+
+    # the reference packer (lib/Tools/Packer/packer.cc), between exact fields and packed floats
+    def _f32(self, n):
+        return np.zeros(n, np.float32)
+
+    def pk_gauge(self):
+        out = self._f32(2 * 12 * 4 * self.V)
+        self.lib.ref_pk_gauge(_fp(out))
+        return out
+
+    def unpk_gauge(self, pk):
+        self.lib.ref_unpk_gauge(_fp(np.ascontiguousarray(pk, np.float32)))
+        return self.get_links()
+
+    def pk_chi(self):
+        out = self._f32(6 * self.Vh * self.no_ps * 2)
+        self.lib.ref_pk_chi(_fp(out))
+        return out
+
+    def unpk_chi(self, pk):
+        self.lib.ref_unpk_chi(_fp(np.ascontiguousarray(pk, np.float32)))
+        return self.get_chi()
+
+    def pk_fermion(self, x):
+        out = self._f32(6 * self.Vh)
+        self.lib.ref_pk_fermion(_fp(out), _dp(np.ascontiguousarray(x, np.complex128)))
+        return out
+
+    def pk_fermion_d(self, x):
+        out = self._f32(6 * self.Vh * 2)
+        self.lib.ref_pk_fermion_d(_fp(out), _dp(np.ascontiguousarray(x, np.complex128)))
+        return out
+
+    def unpk_fermion_d(self, pk):
+        out = np.zeros((self.Vh, 3), np.complex128)
+        self.lib.ref_unpk_fermion_d(_dp(out), _fp(np.ascontiguousarray(pk, np.float32)))
+        return out
+
+    def unpk_shifted(self, pk, order):
+        self.lib.ref_unpk_shifted(_fp(np.ascontiguousarray(pk, np.float32)), order)
+        return self.get_shifted(order)
+
+    def pk_ipdot(self):
+        out = self._f32(8 * 4 * self.V)
+        self.lib.ref_pk_ipdot(_fp(out))
+        return out
+
+    def unpk_ipdot(self, pk):
+        self.lib.ref_unpk_ipdot(_fp(np.ascontiguousarray(pk, np.float32)))
+        return self.get_ipdot()
+
+    def pk_momenta(self):
+        out = self._f32(8 * 4 * self.V)
+        self.lib.ref_pk_momenta(_fp(out))
+        return out
+
+    def unpk_momenta(self, pk):
+        self.lib.ref_unpk_momenta(_fp(np.ascontiguousarray(pk, np.float32)))
+        return self.get_momenta()
+
+    def shift_table(self):
+        t = np.zeros(8 * self.V, np.int32)
+        self.lib.ref_shift_table(_ip(t))
+        return t
 
     def tables(self):
         t = np.zeros(8 * self.V, np.int32)

@@ -528,6 +528,10 @@ void cuda_momenta_sum_multiply(float step)
 }
 
 // cuda_find_max / cuda_find_min (cuda_find_min_max.cu:69-222): start from simple_fermion_packed
+// The start vector of the power iterations: findminmax packs it with the single-precision
+// smartpack_fermion (findminmax.cc:161, packer.cc:156-190), which fills only the first 6*sizeh
+// floats of simple_fermion_packed, and cuda_find_max/min copy only those (cuda_find_min_max.cu:
+// 97-99, 172-174); whatever the rest of the buffer holds is not part of the vector.
 static void start_vector(std::vector<double> &start)
 {
     const long Vh = g_ctx->Vh, V = 2 * Vh;
@@ -535,8 +539,8 @@ static void start_vector(std::vector<double> &start)
     start.assign(6 * Vh, 0.0);
     for (long i = 0; i < Vh; i++)
         for (int c = 0; c < 3; c++) {
-            start[(i * 3 + c) * 2] = (double)pk[2 * i + c * V] + (double)pk[3 * V + 2 * i + c * V];
-            start[(i * 3 + c) * 2 + 1] = (double)pk[2 * i + c * V + 1] + (double)pk[3 * V + 2 * i + c * V + 1];
+            start[(i * 3 + c) * 2] = (double)pk[2 * i + c * V];
+            start[(i * 3 + c) * 2 + 1] = (double)pk[2 * i + c * V + 1];
         }
 }
 

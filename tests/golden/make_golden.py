@@ -105,15 +105,47 @@ def make(tag, coeffs):
     print(tag, "written", {k: (v.shape if hasattr(v, "shape") else v) for k, v in out.items() if k.startswith("traj")})
 
 
+def make_packer(tag):
+    """The reference packer (lib/Tools/Packer/packer.cc, compiled unmodified into the harness as
+    refpk_*) on the fixture fields of ref_<tag>.npz: every packed host format the GPU entry
+    points exchange, and the reference's unpacking of packed buffers."""
+    import oracle
+    g = dict(np.load(os.path.join(HERE, "ref_%s.npz" % tag)))
+    ref = oracle.RefLib(tag)
+    out = {}
+    ref.set_links(g["u"])
+    out["pk_gauge"] = ref.pk_gauge()
+    ref.set_chi(g["chi"])
+    out["pk_chi"] = ref.pk_chi()
+    out["pk_fermion"] = ref.pk_fermion(g["x"])
+    out["pk_fermion_d"] = ref.pk_fermion_d(g["x"])
+    ref.set_ipdot(g["ipdot_full"])
+    out["pk_tamatrix"] = ref.pk_ipdot()
+    ref.set_momenta(g["P"])
+    out["pk_thmatrix"] = ref.pk_momenta()
+    out["shift_table"] = ref.shift_table()
+    # unpacking: of the packed buffers above (the gauge one with its unitarize_with_eta)
+    out["unpk_gauge"] = ref.unpk_gauge(out["pk_gauge"])
+    out["unpk_chi"] = ref.unpk_chi(out["pk_chi"])
+    out["unpk_fermion_d"] = ref.unpk_fermion_d(out["pk_fermion_d"])
+    out["unpk_tamatrix"] = ref.unpk_ipdot(out["pk_tamatrix"])
+    out["unpk_thmatrix"] = ref.unpk_momenta(out["pk_thmatrix"])
+    np.savez_compressed(os.path.join(HERE, "ref_%s_packer.npz" % tag), **out)
+    print(tag, "packer fixture written", sorted(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--build", action="store_true", help="(re)build the reference harness first")
+    ap.add_argument("--packer-only", action="store_true", help="only the packed-format fixture")
     a = ap.parse_args()
     if a.build:
         subprocess.check_call([sys.executable, os.path.join(ROOT, "oracle", "build_ref.py"), "t4", "a6448"])
-    coeffs = coefficients()
-    for tag in ("t4", "a6448"):
-        make(tag, coeffs)
+    if not a.packer_only:
+        coeffs = coefficients()
+        for tag in ("t4", "a6448"):
+            make(tag, coeffs)
+    make_packer("t4")
 
 
 if __name__ == "__main__":

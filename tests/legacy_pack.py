@@ -68,6 +68,12 @@ def unpack_multifermion(pk, nps, Vh):
     return f
 
 
+def pack_fermion(x):
+    """smartpack_fermion (packer.cc:156-190): one (Vh, 3) spinor -> float[6*Vh], single precision
+    (the hi block of pack_fermion_d); findminmax.cc:161 packs the power-iteration start with it."""
+    return pack_multifermion(x[None])[:6 * x.shape[0]]
+
+
 def pack_fermion_d(x):
     """smartpack_fermion_d (packer.cc:192-230): one (Vh, 3) spinor -> float[6*Vh*2]."""
     return pack_multifermion(x[None])
@@ -108,14 +114,16 @@ def unpack_alg(pk, V, antiherm):
         a01 = v[mu, 0, :, 0] + 1j * v[mu, 0, :, 1]
         a02 = v[mu, 0, :, 2] + 1j * v[mu, 0, :, 3]
         a12 = v[mu, 1, :, 0] + 1j * v[mu, 1, :, 1]
-        d0, d1 = v[mu, 1, :, 2], v[mu, 1, :, 3]
+        # diagonal entries built as complex(0, d) / complex(d, 0) and a22 = -a00 - a11 in complex
+        # arithmetic, as the reference does, so that even the signs of zeros agree
+        m00, m11 = np.zeros(V, np.complex128), np.zeros(V, np.complex128)
         if antiherm:
-            m[s, 0, 0], m[s, 1, 1] = 1j * d0, 1j * d1
-            m[s, 2, 2] = -m[s, 0, 0] - m[s, 1, 1]
+            m00.imag, m11.imag = v[mu, 1, :, 2], v[mu, 1, :, 3]
             m[s, 1, 0], m[s, 2, 0], m[s, 2, 1] = -np.conj(a01), -np.conj(a02), -np.conj(a12)
         else:
-            m[s, 0, 0], m[s, 1, 1] = d0, d1
-            m[s, 2, 2] = -d0 - d1
+            m00.real, m11.real = v[mu, 1, :, 2], v[mu, 1, :, 3]
             m[s, 1, 0], m[s, 2, 0], m[s, 2, 1] = np.conj(a01), np.conj(a02), np.conj(a12)
+        m[s, 0, 0], m[s, 1, 1] = m00, m11
+        m[s, 2, 2] = -m00 - m11
         m[s, 0, 1], m[s, 0, 2], m[s, 1, 2] = a01, a02, a12
     return m
