@@ -193,20 +193,27 @@ def run_reference_arm(a):
 MS_DIMS = (24, 24, 24, 32)
 
 
-def msolve_bench(rb, F, np, torch, rank, dev, stream, nrhs=4, nshift=16, res=1e-10):
+def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False, nrhs=4, nshift=16, res=1e-10, only=()):
+    """Multi-shift CG, am=0.01: 16 poles log-spaced in [1e-4, 50], 4 Gaussian RHS, true residual
+    1e-10 for every (RHS, pole) system: absolute |b - (M^dag M + s) x| <= 1e-10 (the reference's
+    stopping criterion, inverter.cc:287) or, with relative, <= 1e-10 |b| (at 32^4 the absolute
+    1e-10 is below the FP64 rounding floor of the smallest poles).  Plain FP64 single-RHS (the
+    reference algorithm, RHS after RHS, then FP64 CG refinement of every system whose FP64 true
+    residual is still above target) against the mixed batched solver; both checked by FP64 true
+    residuals.  The reference algorithm without the refinement is reported too (it stops on its
+    iterated residual).  Every variant runs once untimed, then timed."""
     from rhmc_b200 import replicas as RP
-    """Multi-shift CG at 24^3x32, am=0.01: 16 poles log-spaced in [1e-4, 50], 4 Gaussian RHS,
-    true residual 1e-10.  Plain FP64 single-RHS (the reference algorithm, RHS after RHS, then
-    FP64 CG refinement of every system whose FP64 true residual is still above 1e-10) against
-    the mixed batched solver; both checked by FP64 true residuals.  The reference algorithm
-    without the refinement is reported too (it stops on its iterated residual)."""
-    ctx = rb.Context(MS_DIMS, mass=0.01, beta=5.7, device=dev.index or 0)
+    dims = dims or MS_DIMS
+    ctx = rb.Context(dims, mass=0.01, beta=5.7, device=dev.index or 0)
     ctx.set_stream(stream.cuda_stream)
-    u = F.random_links(MS_DIMS, seed=RP.replica_seed(1001, rank))
+    u = F.random_links(dims, seed=RP.replica_seed(1001, rank))
     ctx.set_gauge(u)
     Vh = ctx.Vh
     shifts = 1e-4 * (5e5) ** (np.arange(nshift) / (nshift - 1.0))
-    b_host = F.random_spinor(MS_DIMS, seed=RP.replica_seed(2002, rank), n=nrhs)
+    b_host = F.random_spinor(dims, seed=RP.replica_seed(2002, rank), n=nrhs)
+    res_target = res
+    if relative:
+        res = res * float(np.sqrt(min((np.abs(bb) ** 2).sum() for bb in b_host)))
     b = torch.zeros(nrhs * 6 * Vh, dtype=torch.float64, device=dev)
     ctx.spinor_to_internal(rb.LINKS_F64_18, b, b_host, nrhs)
     x = torch.zeros(nrhs * nshift * 6 * Vh, dtype=torch.float64, device=dev)
@@ -215,27 +222,38 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, nrhs=4, nshift=16, res=1e-
                                            ("fp64_single_rhs_uncertified", rb.MSOLVE_FP64, rb.LINKS_F64_18, False, 0),
                                            ("mixed_batched", rb.MSOLVE_MIXED, rb.LINKS_F64_12, True, 0),
                                            ("mixed_batched_f32_bulk", rb.MSOLVE_MIXED, rb.LINKS_F32_12, True, 0)):
-        # warm-up on a loose residual (graphs, derived link formats)
-        ctx.msolve(x, b, shifts, 1e-4, nrhs=nrhs if batched else 1, mode=mode, fmt=fmt)
+        if only and name not in only:
+            continue
+        def solve():
+            infos = []
+            if batched:
+                infos.append(ctx.msolve(x, b, shifts, res, nrhs=nrhs, mode=mode, fmt=fmt))
+            else:
+                for r in range(nrhs):
+                    infos.append(ctx.msolve(x[r * nshift * 6 * Vh:], b[r * 6 * Vh:], shifts, res, nrhs=1, mode=mode,
+                                            fmt=fmt, certify=cert))
+            return infos
+
+        # warm-up: the identical solve, untimed (module loading, graphs, workspaces, derived links)
+        solve()
         stream.synchronize()
         t0 = time.perf_counter()
-        infos = []
-        if batched:
-            infos.append(ctx.msolve(x, b, shifts, res, nrhs=nrhs, mode=mode, fmt=fmt))
-        else:
-            for r in range(nrhs):
-                infos.append(ctx.msolve(x[r * nshift * 6 * Vh:], b[r * 6 * Vh:], shifts, res, nrhs=1, mode=mode, fmt=fmt,
-                                        certify=cert))
+        infos = solve()
         stream.synchronize()
         dt = time.perf_counter() - t0
         tr = ctx.true_residuals(x, b, shifts, nrhs=nrhs)
         out[name] = {"s_per_solve": round(dt, 4), "max_true_residual": float(tr.max()),
                      "iters": [i["iters"][0] for i in infos] if not batched else infos[0]["iters"][:nrhs],
                      "refine_iters": sum(i["refine_iters"] for i in infos),
+                     "s_phase_a": round(sum(i["seconds_phase_a"] for i in infos), 4),
+                     "systems_refined": sum(i["systems_refined"] for i in infos),
                      "links": rb.FMT_NAMES[fmt]}
-    out["speedup_mixed_vs_fp64"] = round(out["fp64_single_rhs"]["s_per_solve"] / out["mixed_batched"]["s_per_solve"], 3)
-    out["config"] = {"lattice": list(MS_DIMS), "mass": 0.01, "nshift": nshift, "shifts": [float(shifts[0]), float(shifts[-1])],
-                     "nrhs": nrhs, "residual": res, "links": "Haar (beta=5.7 labels the run)"}
+    if "fp64_single_rhs" in out and "mixed_batched" in out:
+        out["speedup_mixed_vs_fp64"] = round(out["fp64_single_rhs"]["s_per_solve"] / out["mixed_batched"]["s_per_solve"], 3)
+    out["config"] = {"lattice": list(dims), "mass": 0.01, "nshift": nshift, "shifts": [float(shifts[0]), float(shifts[-1])],
+                     "nrhs": nrhs, "residual": res_target,
+                     "residual_kind": "relative to |b| (absolute %.3g)" % res if relative else "absolute",
+                     "links": "Haar (beta=5.7 labels the run)"}
     ctx.close()
     return out
 
@@ -337,8 +355,15 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
     kern["mom_update"] = (_timed(torch, stream, lambda: ctx.mom_update(0.0), reps), 4 * V * 3 * 64)
     kern["link_update"] = (_timed(torch, stream, lambda: ctx.link_update(0.0), reps), 4 * V * (64 + 2 * 144))
     peak, _ = load_peaks()
+    fp64_peak = ctx.fma_peak(True)
     out["kernels"] = {k: {"ms": round(t, 4), "alg_bytes": b, "gbs": round(b / (t * 1e-3) / 1e9, 1),
                           "frac": round(b / (t * 1e-3) / 1e9 / peak, 4)} for k, (t, b) in kern.items()}
+    # the FP64 CUDA-core roofline of the compute-leaning kernels (algorithmic flops per link)
+    for k, fl in (("gauge_force", 2700), ("link_update", 1300)):
+        tf = fl * 4 * V / (kern[k][0] * 1e-3) / 1e12
+        out["kernels"][k].update({"flops_per_link": fl, "tflops": round(tf, 2), "frac_fp64": round(tf / fp64_peak, 4)})
+    out["kernels"]["fp64_fma_peak_tflops"] = round(fp64_peak, 2)
+    out["kernels"]["fp32_fma_peak_tflops"] = round(ctx.fma_peak(False), 2)
     out["kernels"]["note"] = ("fermion_force = D_oe of the 30 vectors batched 8 per link read, then the outer-product/TA "
                               "kernel; bytes: links + ipdot read-modify-write, links once per 8 vectors, per vector "
                               "the spinor in/out of D_oe and the x and h reads of the force kernel")
@@ -464,13 +489,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dims", default="32,32,32,32")
     ap.add_argument("--no-msolve", action="store_true")
-    ap.add_argument("--workload", default="dslash", choices=["dslash", "nf2p1"],
+    ap.add_argument("--workload", default="dslash", choices=["dslash", "nf2p1", "msolve"],
                     help="dslash: the headline line (Dslash + multi-shift CG); nf2p1: N_f=2+1 forces, "
-                         "finite-difference check and trajectories")
+                         "finite-difference check and trajectories; msolve: the multi-shift CG comparison alone")
+    ap.add_argument("--ms-relative", action="store_true", help="msolve workload: residual relative to |b|")
+    ap.add_argument("--ms-variants", default="", help="msolve workload: comma-separated subset of the variants")
     ap.add_argument("--fd-links", type=int, default=16)
     ap.add_argument("--fd-dirs", type=int, default=8)
     ap.add_argument("--nf-steps", type=int, default=20)
     ap.add_argument("--nf-start", default="near1", choices=["haar", "near1"])
+    ap.add_argument("--ms-dims", default="24,24,24,32", help="lattice of the multi-shift CG comparison")
     a = ap.parse_args()
     a.warmup = max(3, a.warmup)
     if a.impl == "reference":
@@ -482,8 +510,9 @@ def main():
     from rhmc_b200 import fields as F
     from rhmc_b200 import replicas as RP
 
-    global DIMS
+    global DIMS, MS_DIMS
     DIMS = tuple(int(v) for v in a.dims.split(","))
+    MS_DIMS = tuple(int(v) for v in a.ms_dims.split(","))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -495,6 +524,17 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+
+    if a.workload == "msolve":
+        stream = torch.cuda.Stream(device=dev)
+        only = [v for v in a.ms_variants.split(",") if v]
+        res = msolve_bench(rb, F, np, torch, rank, dev, stream, relative=a.ms_relative, only=only)
+        if rank == 0:
+            print(json.dumps({"workload": "msolve", "n_gpus": world, "data": "synthetic", **res}))
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     if a.workload == "nf2p1":
         stream = torch.cuda.Stream(device=dev)
@@ -581,12 +621,16 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_gbs = world * 2 * half_dslash_bytes(0, Vh) * e2e_steps / e2e_s / 1e9
 
-    ms = None
+    ms = ms32 = None
     if not a.no_msolve:
         try:
             ms = msolve_bench(rb, F, np, torch, rank, dev, stream)
         except Exception as e:  # reported in the JSON line, the Dslash numbers stand
             ms = {"error": str(e)[:300]}
+        try:
+            ms32 = msolve_bench(rb, F, np, torch, rank, dev, stream, dims=(32, 32, 32, 32), relative=True)
+        except Exception as e:
+            ms32 = {"error": str(e)[:300]}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -620,6 +664,7 @@ def main():
             "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s", "h2d_bytes_per_step": 2 * 48 * Vh,
                     "d2h_bytes_per_step": 2 * 48 * Vh, "api": "rhmc_dslash_host (host spinors, pinned)"},
             "msolve": ms,
+            "msolve_32": ms32,
             "cpu_baseline": cpu,
             "gpu_launches": r["launches"],
             "clocks": r["clocks"],

@@ -147,6 +147,8 @@ typedef struct {
     long refine_iters;     /* mixed mode: batched refinement iterations (sum over batches) */
     int reliable_updates;  /* mixed mode: FP64 residual recomputations */
     double seconds;        /* wall time of the call */
+    double seconds_phase_a;/* mixed mode / certified FP64: wall time of the multi-shift phase */
+    int systems_refined;   /* mixed mode / certified FP64: (rhs, shift) systems that needed refinement */
 } rhmc_msolve_info;
 
 /* (M^dag M + sigma_i) x_{r,i} = b_r for every shift i and RHS r (cuda_shifted_inverter /
@@ -256,6 +258,11 @@ int rhmc_update(rhmc_ctx *ctx, double uniform, int *acc, double *delta_s);
 int rhmc_save_conf(rhmc_ctx *ctx);
 int rhmc_copy_saved(rhmc_ctx *ctx);
 int rhmc_driver_stats(rhmc_ctx *ctx, long *force_evals, long *solves);
+
+/* CUDA-core FMA throughput of this GPU in TFLOP/s (fp64 = 1: FP64, 0: FP32), measured by a
+ * microbenchmark (8 independent FMA chains per thread, 8 blocks of 256 threads per SM, CUDA
+ * events): the compute roofline of the FP64 gauge force and link exponentiation. */
+int rhmc_fma_peak(rhmc_ctx *ctx, int fp64, double *tflops);
 
 /* No counterpart in the reference.  The same values as rhmc_true_residuals, for callers that
  * cannot allocate device memory where they check their solutions (for example while recording

@@ -7,7 +7,8 @@ namespace rhmc {
 
 bool fmt_is_f64(int fmt) { return fmt == RHMC_LINKS_F64_18 || fmt == RHMC_LINKS_F64_12; }
 
-int dslash_grid(rhmc_ctx *c) { return grid_for(c->Vh, DSLASH_BLOCK); }
+// the largest Dslash grid of any configuration (sizes the per-block reduction partials)
+int dslash_grid(rhmc_ctx *c) { return grid_for(c->Vh, DSLASH_MIN_BLOCK); }
 
 template <class LF, int NR>
 static void run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in, size_t stride, const void *y,
@@ -32,9 +33,10 @@ static void run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in,
     a.stop = nullptr;
     a.stop_set = nullptr;
     a.run_if = nullptr;
-    const int grid = dslash_grid(c);
-    if (y) dslash_kernel<LF, NR, true, false, NoFin><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
-    else dslash_kernel<LF, NR, false, false, NoFin><<<grid, DSLASH_BLOCK, 0, c->stream>>>(a);
+    constexpr int B = DslashCfg<LF, NR, false>::block;
+    const int grid = grid_for(c->Vh, B);
+    if (y) dslash_kernel<LF, NR, true, false, NoFin><<<grid, B, 0, c->stream>>>(a);
+    else dslash_kernel<LF, NR, false, false, NoFin><<<grid, B, 0, c->stream>>>(a);
     c->launches++;
 }
 

@@ -17,7 +17,21 @@
 
 namespace rhmc {
 
-constexpr int DSLASH_BLOCK = 256;
+// Threads per block and the minimum resident blocks per SM handed to the register allocator,
+// per link precision, RHS count and epilogue (RED: the solver's fused reductions).  A thread
+// carries NR accumulators and NR neighbour spinors, so wide FP64 batches need many registers;
+// the pair trades registers (spills) against resident warps (latency hiding).  The values are
+// the fastest of the sweep in tune/dslash_tune.cu on B200 at 24^3x32 and 32^4.
+template <class LF, int NR, bool RED>
+struct DslashCfg {
+    static constexpr bool f64 = sizeof(typename LF::real) == 8;
+    static constexpr bool narrow = f64 && (NR == 3 || (NR == 4 && !RED) || NR >= 8);
+    static constexpr int block = narrow ? 128 : 256;
+    static constexpr int minb = (f64 && NR >= 8) ? 2 : (narrow ? 3 : 2);
+};
+
+// the largest grid any configuration launches (for sizing per-block reduction partials)
+constexpr int DSLASH_MIN_BLOCK = 128;
 
 template <class LF, int NR, class FIN = NoFin>
 struct DslashArgs {
@@ -41,8 +55,9 @@ struct DslashArgs {
     const int *run_if;  // optional: skip the launch when *run_if == 0
 };
 
-template <class LF, int NR, bool HAS_Y, bool RED, class FIN>
-__global__ void __launch_bounds__(DSLASH_BLOCK) dslash_kernel(DslashArgs<LF, NR, FIN> a)
+template <class LF, int NR, bool HAS_Y, bool RED, class FIN, int BLOCK = DslashCfg<LF, NR, RED>::block,
+          int MINB = DslashCfg<LF, NR, RED>::minb>
+__global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, FIN> a)
 {
     typedef typename LF::real R;
     if (a.stop && *(volatile const int *)a.stop) {

@@ -7,8 +7,9 @@
 //   fermion_force_kernel TA(U F_f) with F_f the outer products of fermionforce
 //                        (lib/Action/fermionforce.cc:46-104): even x: sum a_i h_i(x+mu) (x) x_i(x)^*,
 //                        odd x: -sum a_i x_i(x+mu) (x) h_i(x)^*, h_i = Doe x_i (with its 1/2).
-// One thread per link, mu fastest inside a site (the four links of a site share the site's
-// loads through L1).  All shifted solutions of all right-hand sides are summed in registers,
+// gauge_force_kernel runs one thread per site for a fixed mu (blockIdx.y); fermion_force_kernel
+// one thread per link, mu fastest inside a site (the four links of a site share the site's
+// spinor loads through L1).  All shifted solutions of all right-hand sides are summed in registers,
 // so the 18-real force matrix never goes to HBM (the reference GPU code read-modify-writes an
 // 18 x 4V float buffer once per shift, lib/Cuda/cuda_fermion_force.cu:370-386).
 #include <vector>
@@ -35,6 +36,8 @@ __device__ __forceinline__ int hidx(const Geom &g, const Site &s) { return half_
 
 // S_mu(x) = sum_{nu != mu} [ U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
 //                          + U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu) ]
+// Each staple is formed row by row (one row of the two-link product live at a time), with the
+// same operation order per element as a full product followed by a sum.
 __device__ M3 staple_sum(const Geom &g, const double2 *__restrict__ U, int mu, int p, const Site &s)
 {
     const int Vh = g.Vh, q = 1 - p;
@@ -45,25 +48,69 @@ __device__ M3 staple_sum(const Geom &g, const double2 *__restrict__ U, int mu, i
     for (int nu = 0; nu < 4; nu++) {
         if (nu == mu) continue;
         const Site xpn = shifted(g, s, nu, +1), xmn = shifted(g, s, nu, -1), xpmmn = shifted(g, xpm, nu, -1);
-        M3 a = m3_mul_nd(load_link64(U, Vh, nu, q, kxpm), load_link64(U, Vh, mu, q, hidx(g, xpn)));
-        a = m3_mul_nd(a, load_link64(U, Vh, nu, p, kx));
-        m3_add(S, a);
-        const int kxmn = hidx(g, xmn);
-        const M3 ba = m3_mul(load_link64(U, Vh, mu, q, kxmn), load_link64(U, Vh, nu, p, hidx(g, xpmmn)));
-        m3_add(S, m3_mul_dn(ba, load_link64(U, Vh, nu, q, kxmn)));
+        {
+            // upper: (U_nu(x+mu) U_mu(x+nu)^dag) U_nu(x)^dag
+            const M3 A = load_link64(U, Vh, nu, q, kxpm), B = load_link64(U, Vh, mu, q, hidx(g, xpn));
+            const M3 Cm = load_link64(U, Vh, nu, p, kx);
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                C t[3];
+#pragma unroll
+                for (int l = 0; l < 3; l++) {
+                    C v = A.e[i][0] * conj(B.e[l][0]);
+                    v = v + A.e[i][1] * conj(B.e[l][1]);
+                    v = v + A.e[i][2] * conj(B.e[l][2]);
+                    t[l] = v;
+                }
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    C v = t[0] * conj(Cm.e[j][0]);
+                    v = v + t[1] * conj(Cm.e[j][1]);
+                    v = v + t[2] * conj(Cm.e[j][2]);
+                    S.e[i][j] = S.e[i][j] + v;
+                }
+            }
+        }
+        {
+            // lower: (U_mu(x-nu) U_nu(x+mu-nu))^dag U_nu(x-nu)
+            const int kxmn = hidx(g, xmn);
+            const M3 A = load_link64(U, Vh, mu, q, kxmn), B = load_link64(U, Vh, nu, p, hidx(g, xpmmn));
+            const M3 Cm = load_link64(U, Vh, nu, q, kxmn);
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                C col[3];  // column i of A B
+#pragma unroll
+                for (int l = 0; l < 3; l++) {
+                    C v = A.e[l][0] * B.e[0][i];
+                    v = cmadd(A.e[l][1], B.e[1][i], v);
+                    v = cmadd(A.e[l][2], B.e[2][i], v);
+                    col[l] = v;
+                }
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    C v = conj(col[0]) * Cm.e[0][j];
+                    v = v + conj(col[1]) * Cm.e[1][j];
+                    v = v + conj(col[2]) * Cm.e[2][j];
+                    S.e[i][j] = S.e[i][j] + v;
+                }
+            }
+        }
     }
     return S;
 }
 
-// mode 0: ipdot = TA(U beta/3 S); mode 1: ipdot += TA(U beta/3 S)
-__global__ void __launch_bounds__(FORCE_BLOCK) gauge_force_kernel(Geom g, const double2 *__restrict__ U, double *IP,
-                                                                   double beta_by_three, int mode)
+// mode 0: ipdot = TA(U beta/3 S); mode 1: ipdot += TA(U beta/3 S).
+// One thread per site of both parities, blockIdx.y = mu: a warp covers 32 consecutive sites of
+// one parity, so every link-plane load of the warp is one contiguous 512-byte segment (own
+// links) or nearly so (neighbour links).  At 3 resident blocks per SM the register budget is
+// 170 per thread with no spills.
+__global__ void __launch_bounds__(FORCE_BLOCK, 3) gauge_force_kernel(Geom g, const double2 *__restrict__ U, double *IP,
+                                                                      double beta_by_three, int mode)
 {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int mu = blockIdx.y;
+    const long site = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const int Vh = g.Vh;
-    if (t >= 8L * Vh) return;
-    const int mu = (int)(t & 3);
-    const long site = t >> 2;
+    if (site >= 2L * Vh) return;
     const int p = site >= Vh;
     const int k = (int)(site - (long)p * Vh);
     const Site s = site_of(g, p, k);
@@ -133,8 +180,8 @@ __global__ void __launch_bounds__(FORCE_BLOCK) fermion_force_kernel(Geom g, cons
 
 int gauge_force(rhmc_ctx *c, int mode)
 {
-    const long n = 8L * c->Vh;
-    gauge_force_kernel<<<grid_for(n, FORCE_BLOCK), FORCE_BLOCK, 0, c->stream>>>(c->g, c->U64, c->IP, c->beta / 3.0, mode);
+    const dim3 grid((unsigned)grid_for(2L * c->Vh, FORCE_BLOCK), 4);
+    gauge_force_kernel<<<grid, FORCE_BLOCK, 0, c->stream>>>(c->g, c->U64, c->IP, c->beta / 3.0, mode);
     c->launches++;
     CK(cudaGetLastError());
     return RHMC_OK;

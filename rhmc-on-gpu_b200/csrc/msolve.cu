@@ -32,9 +32,10 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     CK(c->ws.get("ms_s", NR * vbytes, &s));
     CK(c->ws.get("ms_ps", (size_t)NR * S * vbytes, &ps));
     CK(c->ws.get("ms_state", sizeof(MSState), &stv));
-    const int gd = dslash_grid(c), gv = vec_grid(c);
-    const int gmax = gd > gv ? gd : gv;
-    CK(c->ws.get("ms_partials", (size_t)gmax * 2 * NR * sizeof(double), &part));
+    const int gv = vec_grid(c);
+    // the grids of this configuration's two Dslash launches
+    const int gd1 = grid_for(Vh, DslashCfg<LF, NR, false>::block), gd2 = grid_for(Vh, DslashCfg<LF, NR, true>::block);
+    CK(c->ws.get("ms_partials", (size_t)red_chunks(Vh) * 2 * NR * sizeof(double), &part));
     CK(c->ws.get("ms_tickets", 4 * sizeof(unsigned), &tick));
     int *hflag = c->hflags;
     MSState *st = (MSState *)stv;
@@ -95,8 +96,8 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     cudaGraphExec_t exec;
     CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < chunk; it++) {
-        dslash_kernel<LF, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(a1);
-        dslash_kernel<LF, NR, true, true, FinAlpha<NR>><<<gd, DSLASH_BLOCK, 0, s_>>>(a2);
+        dslash_kernel<LF, NR, false, false, NoFin><<<gd1, DslashCfg<LF, NR, false>::block, 0, s_>>>(a1);
+        dslash_kernel<LF, NR, true, true, FinAlpha<NR>><<<gd2, DslashCfg<LF, NR, true>::block, 0, s_>>>(a2);
         ms_resid_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)r, (const E *)s, pt, tk + 2, st);
         ms_update_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, S, stride, (const E *)r, (E *)p, (E *)ps, xs, st);
     }

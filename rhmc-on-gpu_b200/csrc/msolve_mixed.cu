@@ -276,8 +276,8 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     CK(c->ws.get("rb_h64", NR * v64, &h64));
     CK(c->ws.get("rb_t64", NR * v64, &t64));
     CK(c->ws.get("rb_state", sizeof(RBState), &stv));
-    const int gd = dslash_grid(c), gv = grid_for(Vh, VEC_BLOCK);
-    CK(c->ws.get("rb_partials", (size_t)(gd > gv ? gd : gv) * 2 * NR * sizeof(double), &part));
+    const int gv = grid_for(Vh, VEC_BLOCK);
+    CK(c->ws.get("rb_partials", (size_t)red_chunks(Vh) * 2 * NR * sizeof(double), &part));
     CK(c->ws.get("rb_tickets", 4 * sizeof(unsigned), &tick));
     L64_18 l64;
     links_f64_18(c, &l64);
@@ -327,13 +327,16 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     cudaGraphExec_t exec;
     CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
     rb_accum_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (E *)xs, st);
-    dslash_kernel<L64_18, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(d1);
-    dslash_kernel<L64_18, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(d2);
+    constexpr int B64 = DslashCfg<L64_18, NR, false>::block, BS1 = DslashCfg<LF, NR, false>::block,
+                  BS2 = DslashCfg<LF, NR, true>::block;
+    const int g64 = grid_for(Vh, B64), gs1 = grid_for(Vh, BS1), gs2 = grid_for(Vh, BS2);
+    dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d1);
+    dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d2);
     rb_resid_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, bg, xg, (const double2 *)t64, (E *)rs, (E *)p, co,
                                                          pt, tk, st);
     for (int it = 0; it < n_ru; it++) {
-        dslash_kernel<LF, NR, false, false, NoFin><<<gd, DSLASH_BLOCK, 0, s_>>>(s1);
-        dslash_kernel<LF, NR, true, true, FinRBAlpha<NR>><<<gd, DSLASH_BLOCK, 0, s_>>>(s2);
+        dslash_kernel<LF, NR, false, false, NoFin><<<gs1, BS1, 0, s_>>>(s1);
+        dslash_kernel<LF, NR, true, true, FinRBAlpha<NR>><<<gs2, BS2, 0, s_>>>(s2);
         rb_xr_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)xs, (E *)rs, (const E *)p, (const E *)ap, pt, tk + 2, st);
         rb_p_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)rs, (E *)p, st);
     }
@@ -404,7 +407,7 @@ static int rb_group_n(rhmc_ctx *c, const LF &lf, int n, const double *coef, cons
 template <class LF>
 static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shifts, int nrhs, double res, int max_iter,
                       double2 *x, const double2 *b, long *iters, int *ru, double ru_delta, int max_batch = RB_MAX,
-                      const double *skip_below = nullptr)
+                      const double *skip_below = nullptr, int *nsys = nullptr)
 {
     const size_t stride = 3 * (size_t)c->Vh;
     const size_t v64 = stride * sizeof(double2);
@@ -415,6 +418,7 @@ static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shift
     for (int q = 0; q < nshift * nrhs; q++)
         if (!skip_below || skip_below[q] > res) order.push_back(q);
     std::stable_sort(order.begin(), order.end(), [&](int a, int bq) { return shifts[a % nshift] < shifts[bq % nshift]; });
+    if (nsys) *nsys = (int)order.size();
     const double m2 = c->mass * c->mass;
     size_t g0 = 0;
     while (g0 < order.size()) {
@@ -503,18 +507,22 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
         convert_kernel<float2><<<grid_for(n, 256), 256, 0, c->stream>>>(n, x, (const float2 *)xa);
         c->launches++;
         CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(c->stream));
     }
+    const double t_a = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     long it_b = 0;
-    int ru = 0;
+    int ru = 0, nsys = 0;
     // refinement: FP32 sloppy links of the matching width
     if (fmt == RHMC_LINKS_F32_18 || fmt == RHMC_LINKS_F64_18) {
         L32_18 lf;
         links_f32_18(c, &lf);
-        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX, tr.empty() ? nullptr : tr.data());
+        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX,
+                        tr.empty() ? nullptr : tr.data(), &nsys);
     } else {
         L32_12 lf;
         links_f32_12(c, &lf);
-        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX, tr.empty() ? nullptr : tr.data());
+        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX,
+                        tr.empty() ? nullptr : tr.data(), &nsys);
     }
     CK(cudaStreamSynchronize(c->stream));
     if (info) {
@@ -523,6 +531,8 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
         info->refine_iters = it_b;
         info->reliable_updates = ru;
         info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        info->seconds_phase_a = t_a;
+        info->systems_refined = nsys;
     }
     return rc;
 }
@@ -561,7 +571,9 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, con
         done += n;
     }
     long it_b = 0;
-    int ru = 0;
+    int ru = 0, nsys = 0;
+    cudaStreamSynchronize(c->stream);
+    const double t_a = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (rc == RHMC_OK && P->certify) {
         // FP64 defect correction of every system whose FP64 true residual is above target
         std::vector<double> tr((size_t)P->nshift * P->nrhs);
@@ -570,7 +582,8 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, con
         if (rc == RHMC_OK) {
             L64_18 lf;
             links_f64_18(c, &lf);
-            rc = refine_all(c, lf, P->nshift, P->shifts, P->nrhs, P->residual, P->max_iter, x, b, &it_b, &ru, 0.05, 1, tr.data());
+            rc = refine_all(c, lf, P->nshift, P->shifts, P->nrhs, P->residual, P->max_iter, x, b, &it_b, &ru, 0.05, 1, tr.data(),
+                            &nsys);
         }
         cudaStreamSynchronize(c->stream);
     }
@@ -579,6 +592,8 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, con
         info->refine_iters = it_b;
         info->reliable_updates = ru;
         info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        info->seconds_phase_a = t_a;
+        info->systems_refined = nsys;
     }
     return rc;
 }

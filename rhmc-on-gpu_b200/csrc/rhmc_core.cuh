@@ -289,40 +289,97 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double *smem)
     __syncthreads();
 }
 
-// Grid-wide deterministic reduction: every block writes its N block sums to
-// partials[block][N]; the last block to finish (atomic ticket) re-reads all partials in
-// block order, sums them and hands the totals to fin() in thread 0, then re-arms the ticket.
-// All threads of every block must call it.
+// Grid-wide deterministic reduction whose result does not depend on the launch's block size.
+// Sites are summed in fixed chunks of RED_CHUNK = 128 consecutive threads (4 warps): a warp
+// shuffle tree per warp, then the 4 warp sums in order.  Every block writes one partial per
+// chunk it covers (blockDim must be a multiple of 128); the last block to finish (atomic
+// ticket) sums the chunk partials with its first 128 threads (thread t takes chunks t, t+128,
+// ... in order), then a shuffle tree per warp and the 4 warp sums in order, hands the totals to
+// fin() in thread 0 and re-arms the ticket.  A batched launch (NR right-hand sides, 128-thread
+// blocks) therefore reduces each RHS bit for bit as a single-RHS launch (256-thread blocks) does.
+// All threads of every block must call it.  partials: red_chunks(n) * N doubles.
 struct NoFin {
     __device__ void operator()(const double *) const {}
 };
+
+constexpr int RED_CHUNK = 128;
+
+// number of chunk partials a reduction over n threads may write, for blocks of 128 or 256
+__host__ __device__ __forceinline__ long red_chunks(long n) { return 2 * ((n + 255) / 256); }
 
 template <int N, class FIN>
 __device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials, unsigned *ticket, const FIN &fin)
 {
     __shared__ double smem[N * 32];
     __shared__ int am_last;
-    block_sum<N>(v, smem);
-    if (threadIdx.x == 0) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int cpb = blockDim.x / RED_CHUNK;
 #pragma unroll
-        for (int j = 0; j < N; j++) partials[(size_t)blockIdx.x * N + j] = v[j];
+    for (int j = 0; j < N; j++) v[j] = warp_sum(v[j]);
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < N; j++) smem[j * 32 + wid] = v[j];
+    __syncthreads();
+    if (threadIdx.x < cpb) {
+        const int c = threadIdx.x;
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            double t = smem[j * 32 + 4 * c];
+            t += smem[j * 32 + 4 * c + 1];
+            t += smem[j * 32 + 4 * c + 2];
+            t += smem[j * 32 + 4 * c + 3];
+            partials[((size_t)blockIdx.x * cpb + c) * N + j] = t;
+        }
         __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
         unsigned t = atomicAdd(ticket, 1u);
         am_last = (t == gridDim.x - 1);
     }
     __syncthreads();
     if (!am_last) return;
     __threadfence();
+    const int nch = (int)gridDim.x * cpb;
     double acc[N];
 #pragma unroll
     for (int j = 0; j < N; j++) acc[j] = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+    if (threadIdx.x < RED_CHUNK) {
+        // chunks t, t+128, ... added in that order; 4 chunks' loads are issued together
+        int i = threadIdx.x;
+        for (; i + 3 * RED_CHUNK < nch; i += 4 * RED_CHUNK) {
+            double q[4][N];
 #pragma unroll
-        for (int j = 0; j < N; j++) acc[j] += __ldcg(partials + (size_t)i * N + j);
-    block_sum<N>(acc, smem);
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int j = 0; j < N; j++) q[u][j] = __ldcg(partials + (size_t)(i + u * RED_CHUNK) * N + j);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int j = 0; j < N; j++) acc[j] += q[u][j];
+        }
+        for (; i < nch; i += RED_CHUNK)
+#pragma unroll
+            for (int j = 0; j < N; j++) acc[j] += __ldcg(partials + (size_t)i * N + j);
+    }
+#pragma unroll
+    for (int j = 0; j < N; j++) acc[j] = warp_sum(acc[j]);
+    if (lane == 0 && wid < 4)
+#pragma unroll
+        for (int j = 0; j < N; j++) smem[j * 32 + wid] = acc[j];
+    __syncthreads();
     if (threadIdx.x == 0) {
+        double tot[N];
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            double t = smem[j * 32];
+            t += smem[j * 32 + 1];
+            t += smem[j * 32 + 2];
+            t += smem[j * 32 + 3];
+            tot[j] = t;
+        }
         *ticket = 0;
-        fin(acc);
+        fin(tot);
     }
 }
 

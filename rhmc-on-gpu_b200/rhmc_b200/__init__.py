@@ -202,11 +202,13 @@ class MsolveParams(ctypes.Structure):
 
 class MsolveInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("iters", ctypes.c_int * 8), ("refine_iters", ctypes.c_long),
-                ("reliable_updates", ctypes.c_int), ("seconds", ctypes.c_double)]
+                ("reliable_updates", ctypes.c_int), ("seconds", ctypes.c_double), ("seconds_phase_a", ctypes.c_double),
+                ("systems_refined", ctypes.c_int)]
 
     def as_dict(self):
         return {"status": self.status, "iters": list(self.iters), "refine_iters": self.refine_iters,
-                "reliable_updates": self.reliable_updates, "seconds": self.seconds}
+                "reliable_updates": self.reliable_updates, "seconds": self.seconds,
+                "seconds_phase_a": self.seconds_phase_a, "systems_refined": self.systems_refined}
 
 
 def _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a=0.0, certify=0, ru_delta=0.0):
@@ -443,3 +445,13 @@ def _find_min(self, start, mx):
 
 Context.find_max = _find_max
 Context.find_min = _find_min
+
+
+def _fma_peak(self, fp64=True):
+    """Measured CUDA-core FMA throughput (TFLOP/s), FP64 or FP32 (rhmc_fma_peak)."""
+    v = ctypes.c_double()
+    self.call("rhmc_fma_peak", int(bool(fp64)), ctypes.byref(v))
+    return v.value
+
+
+Context.fma_peak = _fma_peak
