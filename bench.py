@@ -193,7 +193,8 @@ def run_reference_arm(a):
 MS_DIMS = (24, 24, 24, 32)
 
 
-def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False, nrhs=4, nshift=16, res=1e-10, only=()):
+def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False, nrhs=4, nshift=16, res=1e-10, only=(),
+                 mass=0.01, warmup=True):
     """Multi-shift CG, am=0.01: 16 poles log-spaced in [1e-4, 50], 4 Gaussian RHS, true residual
     1e-10 for every (RHS, pole) system: absolute |b - (M^dag M + s) x| <= 1e-10 (the reference's
     stopping criterion, inverter.cc:287) or, with relative, <= 1e-10 |b| (at 32^4 the absolute
@@ -204,7 +205,7 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False,
     iterated residual).  Every variant runs once untimed, then timed."""
     from rhmc_b200 import replicas as RP
     dims = dims or MS_DIMS
-    ctx = rb.Context(dims, mass=0.01, beta=5.7, device=dev.index or 0)
+    ctx = rb.Context(dims, mass=mass, beta=5.7, device=dev.index or 0)
     ctx.set_stream(stream.cuda_stream)
     u = F.random_links(dims, seed=RP.replica_seed(1001, rank))
     ctx.set_gauge(u)
@@ -235,7 +236,8 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False,
             return infos
 
         # warm-up: the identical solve, untimed (module loading, graphs, workspaces, derived links)
-        solve()
+        if warmup:
+            solve()
         stream.synchronize()
         t0 = time.perf_counter()
         infos = solve()
@@ -250,10 +252,12 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False,
                      "links": rb.FMT_NAMES[fmt]}
     if "fp64_single_rhs" in out and "mixed_batched" in out:
         out["speedup_mixed_vs_fp64"] = round(out["fp64_single_rhs"]["s_per_solve"] / out["mixed_batched"]["s_per_solve"], 3)
-    out["config"] = {"lattice": list(dims), "mass": 0.01, "nshift": nshift, "shifts": [float(shifts[0]), float(shifts[-1])],
+    out["config"] = {"lattice": list(dims), "mass": mass, "nshift": nshift, "shifts": [float(shifts[0]), float(shifts[-1])],
                      "nrhs": nrhs, "residual": res_target,
                      "residual_kind": "relative to |b| (absolute %.3g)" % res if relative else "absolute",
                      "links": "Haar (beta=5.7 labels the run)"}
+    free, total = torch.cuda.mem_get_info(dev)
+    out["device_memory_in_use_gb"] = round((total - free) / 1e9, 2)  # workspaces of all variants, at the end
     ctx.close()
     return out
 
@@ -494,6 +498,10 @@ def main():
                          "finite-difference check and trajectories; msolve: the multi-shift CG comparison alone")
     ap.add_argument("--ms-relative", action="store_true", help="msolve workload: residual relative to |b|")
     ap.add_argument("--ms-variants", default="", help="msolve workload: comma-separated subset of the variants")
+    ap.add_argument("--ms-nrhs", type=int, default=4)
+    ap.add_argument("--ms-nshift", type=int, default=16)
+    ap.add_argument("--ms-mass", type=float, default=0.01)
+    ap.add_argument("--ms-no-warmup", action="store_true", help="msolve workload: time the first solve")
     ap.add_argument("--fd-links", type=int, default=16)
     ap.add_argument("--fd-dirs", type=int, default=8)
     ap.add_argument("--nf-steps", type=int, default=20)
@@ -528,7 +536,9 @@ def main():
     if a.workload == "msolve":
         stream = torch.cuda.Stream(device=dev)
         only = [v for v in a.ms_variants.split(",") if v]
-        res = msolve_bench(rb, F, np, torch, rank, dev, stream, relative=a.ms_relative, only=only)
+        res = msolve_bench(rb, F, np, torch, rank, dev, stream, relative=a.ms_relative, only=only, nrhs=a.ms_nrhs,
+                           nshift=a.ms_nshift, mass=a.ms_mass, warmup=not a.ms_no_warmup)
+
         if rank == 0:
             print(json.dumps({"workload": "msolve", "n_gpus": world, "data": "synthetic", **res}))
         if dist is not None:
