@@ -484,6 +484,76 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
     return out
 
 
+def rhmc4_bench(a, rb, F, np, torch, rank, dev, stream):
+    """Plain RHMC as the reference CPU build runs it: N_f=2 staggered on 4^4, beta=5.5, am=0.1,
+    degree-8 approximations of x^(1/4) (heatbath) and x^(-1/2) (force, action) on [1e-3, 64],
+    Haar hot start (seed 1001), leapfrog tau=1 with 10 steps, FP64, CG residual 1e-10, 5
+    trajectories; momenta (seed 3003+i), pseudofermions (seed 2002+i) and Metropolis uniforms
+    (seed 4004) injected identically into the B200 driver and into the reference's own CPU code
+    (oracle/_ref/libref_t4.so, the unmodified sources behind the harness; its leapfrog kicks with
+    the sign of the wired integrators).  Reports Delta H, acceptance and plaquette per trajectory
+    for both, their largest differences, and seconds per trajectory of each."""
+    from rhmc_b200 import rational as R
+    dims = (4, 4, 4, 4)
+    lo, hi = 1e-3, 64.0 / 1.05  # the rescale widens the top by 1.05: range [1e-3, 64]
+    eps = lo / 64.0
+    ap_ = [R.rational_power(0.25, 8, eps), R.rational_power(-0.5, 8, eps), R.rational_power(-0.5, 8, eps)]
+    ntraj = 5
+    uni = np.random.Generator(np.random.Philox(4004)).random(ntraj)
+    u0 = F.random_links(dims, seed=1001)
+    ctx = rb.Context(dims, mass=0.1, beta=5.5, device=dev.index or 0)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_gauge(u0)
+    ctx.driver_setup(no_flavours=2, no_ps=1, no_md=10, integrator=rb.INT_LEAPFROG, residue_metro=1e-10, residue_md=1e-10)
+    for w in range(3):
+        ctx.set_approx(w, ap_[w])
+    ctx.set_eig_bounds(lo, hi)
+    gpu, t_gpu = [], []
+    for i in range(ntraj):
+        ctx.set_momenta(F.random_momenta(dims, seed=3003 + i))
+        ctx.set_phi(F.random_spinor(dims, seed=2002 + i, n=1))
+        stream.synchronize()
+        t0 = time.perf_counter()
+        de, acc = ctx.update(float(uni[i]))
+        stream.synchronize()
+        t_gpu.append(time.perf_counter() - t0)
+        gpu.append({"delta_H": de, "accepted": acc, "plaquette": list(ctx.plaquette())})
+    u_gpu = ctx.get_gauge()
+    ctx.close()
+    out = {"config": {"lattice": list(dims), "no_flavours": 2, "mass": 0.1, "beta": 5.5, "degree": 8, "range": [lo, 64.0],
+                      "integrator": "leapfrog tau=1, 10 steps", "residual": 1e-10, "trajectories": ntraj,
+                      "approx_max_rel_err": max(c["max_rel_err"] for c in ap_)},
+           "b200": gpu, "b200_s_per_trajectory": round(float(np.median(t_gpu)), 5)}
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        ref = oracle.RefLib("t4")
+    except Exception as e:  # the reference harness is built where the reference sources are
+        out["reference"] = {"unavailable": str(e)[:200]}
+        return out
+    ref.set_links(u0)
+    for w in range(3):
+        ref.set_approx(w, ap_[w])
+    ref.set_minmax(lo, hi)
+    cpu, t_cpu = [], []
+    for i in range(ntraj):
+        ref.set_momenta(F.random_momenta(dims, seed=3003 + i))
+        ref.set_phi(F.random_spinor(dims, seed=2002 + i, n=1))
+        t0 = time.perf_counter()
+        de, acc = ref.trajectory(3, float(uni[i]))
+        t_cpu.append(time.perf_counter() - t0)
+        cpu.append({"delta_H": de, "accepted": acc, "plaquette": list(ref.plaquette())})
+    out["reference"] = cpu
+    out["reference_s_per_trajectory"] = round(float(np.median(t_cpu)), 5)
+    out["reference_cores"] = 1
+    out["max_abs_diff"] = {
+        "delta_H": max(abs(g["delta_H"] - c["delta_H"]) for g, c in zip(gpu, cpu)),
+        "plaquette": max(abs(x - y) for g, c in zip(gpu, cpu) for x, y in zip(g["plaquette"], c["plaquette"])),
+        "acceptance_mismatches": sum(g["accepted"] != c["accepted"] for g, c in zip(gpu, cpu)),
+        "links_after": float(np.abs(u_gpu - ref.get_links()).max())}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -493,7 +563,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dims", default="32,32,32,32")
     ap.add_argument("--no-msolve", action="store_true")
-    ap.add_argument("--workload", default="dslash", choices=["dslash", "nf2p1", "msolve"],
+    ap.add_argument("--workload", default="dslash", choices=["dslash", "nf2p1", "msolve", "rhmc4"],
                     help="dslash: the headline line (Dslash + multi-shift CG); nf2p1: N_f=2+1 forces, "
                          "finite-difference check and trajectories; msolve: the multi-shift CG comparison alone")
     ap.add_argument("--ms-relative", action="store_true", help="msolve workload: residual relative to |b|")
@@ -532,6 +602,16 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+
+    if a.workload == "rhmc4":
+        stream = torch.cuda.Stream(device=dev)
+        res = rhmc4_bench(a, rb, F, np, torch, rank, dev, stream)
+        if rank == 0:
+            print(json.dumps({"workload": "rhmc4", "n_gpus": world, "data": "synthetic", **res}))
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     if a.workload == "msolve":
         stream = torch.cuda.Stream(device=dev)

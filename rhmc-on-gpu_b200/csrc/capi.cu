@@ -100,6 +100,7 @@ int rhmc_destroy(rhmc_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     cudaFree(c->U64); cudaFree(c->U64_12); cudaFree(c->U32_18); cudaFree(c->U32_12);
     cudaFree(c->P); cudaFree(c->IP);
+    c->graphs.release();
     c->ws.release();
     driver_free(c->driver);
     if (c->hflags) cudaFreeHost(c->hflags);

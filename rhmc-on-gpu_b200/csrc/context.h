@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <map>
 #include <string>
+#include <vector>
 
 #include "rhmc_core.cuh"
 #include "../../include/rhmc_b200.h"
@@ -37,6 +38,50 @@ struct Workspace {
     }
 };
 
+// Instantiated CUDA graphs of the solver loops, keyed by everything their kernels capture
+// (pointers, sizes, coefficients, stream), so that a solve repeated with the same buffers and
+// shifts (every force evaluation of a trajectory) replays the graph without re-capturing and
+// re-instantiating it.  Least recently used entries are destroyed beyond `cap`.
+struct GraphCache {
+    struct Entry {
+        std::string key;
+        cudaGraphExec_t exec;
+        unsigned long used;
+    };
+    std::vector<Entry> e;
+    unsigned long tick = 0;
+    size_t cap = 48;
+    cudaGraphExec_t find(const std::string &k)
+    {
+        for (Entry &x : e)
+            if (x.key == k) {
+                x.used = ++tick;
+                return x.exec;
+            }
+        return nullptr;
+    }
+    void put(const std::string &k, cudaGraphExec_t g)
+    {
+        if (e.size() >= cap) {
+            size_t lru = 0;
+            for (size_t i = 1; i < e.size(); i++)
+                if (e[i].used < e[lru].used) lru = i;
+            cudaGraphExecDestroy(e[lru].exec);
+            e.erase(e.begin() + lru);
+        }
+        e.push_back({k, g, ++tick});
+    }
+    void release()
+    {
+        for (Entry &x : e) cudaGraphExecDestroy(x.exec);
+        e.clear();
+    }
+};
+
+// the bytes of a plain-data key (zero-initialise the struct before filling it)
+template <class K>
+inline std::string key_bytes(const K &k) { return std::string(reinterpret_cast<const char *>(&k), sizeof(K)); }
+
 }  // namespace rhmc
 
 struct rhmc_ctx {
@@ -62,6 +107,7 @@ struct rhmc_ctx {
     cudaStream_t aux;
     cudaEvent_t ev_fork, ev_join;
     long launches;  // kernels launched by this context (counted by the host wrappers)
+    rhmc::GraphCache graphs;  // instantiated solver-loop graphs
     rhmc::Driver *driver;  // molecular-dynamics driver state (rhmc_driver_setup), or null
 };
 

@@ -92,20 +92,35 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     a2.stop = &st->stop;
 
     const int chunk = A.chunk > 0 ? A.chunk : 8;
-    cudaGraph_t graph;
-    cudaGraphExec_t exec;
-    CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-    for (int it = 0; it < chunk; it++) {
-        dslash_kernel<LF, NR, false, false, NoFin><<<gd1, DslashCfg<LF, NR, false>::block, 0, s_>>>(a1);
-        dslash_kernel<LF, NR, true, true, FinAlpha<NR>><<<gd2, DslashCfg<LF, NR, true>::block, 0, s_>>>(a2);
-        ms_resid_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)r, (const E *)s, pt, tk + 2, st);
-        ms_update_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, S, stride, (const E *)r, (E *)p, (E *)ps, xs, st);
+    struct Key {
+        int kind, link_reals, link_bytes, nr, chunk, nshift, vh;
+        const void *links, *r, *p, *h, *s, *ps, *xs, *pt, *tk, *st;
+        double alpha;
+        cudaStream_t stream;
+    } key;
+    memset(&key, 0, sizeof(key));
+    key.kind = 1; key.link_reals = LF::reals; key.link_bytes = (int)sizeof(typename LF::real); key.nr = NR;
+    key.chunk = chunk; key.nshift = S; key.vh = Vh; key.links = lf.p; key.r = r; key.p = p; key.h = h; key.s = s;
+    key.ps = ps; key.xs = xs; key.pt = pt; key.tk = tk; key.st = st; key.alpha = (double)a2.alpha; key.stream = s_;
+    const std::string kb = key_bytes(key);
+    cudaError_t ce = cudaSuccess;
+    cudaGraphExec_t exec = c->graphs.find(kb);
+    if (!exec) {
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        for (int it = 0; it < chunk; it++) {
+            dslash_kernel<LF, NR, false, false, NoFin><<<gd1, DslashCfg<LF, NR, false>::block, 0, s_>>>(a1);
+            dslash_kernel<LF, NR, true, true, FinAlpha<NR>><<<gd2, DslashCfg<LF, NR, true>::block, 0, s_>>>(a2);
+            ms_resid_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)r, (const E *)s, pt, tk + 2, st);
+            ms_update_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, S, stride, (const E *)r, (E *)p, (E *)ps, xs, st);
+        }
+        ce = cudaStreamEndCapture(s_, &graph);
+        if (ce != cudaSuccess) return cuda_fail(ce, "msolve capture");
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return cuda_fail(ce, "msolve instantiate");
+        c->graphs.put(kb, exec);
     }
-    cudaError_t ce = cudaStreamEndCapture(s_, &graph);
-    if (ce != cudaSuccess) return cuda_fail(ce, "msolve capture");
-    ce = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ce != cudaSuccess) return cuda_fail(ce, "msolve instantiate");
 
     cudaEvent_t ev[2];
     cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
@@ -129,7 +144,6 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     c->launches += launched * chunk * 4;
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
-    cudaGraphExecDestroy(exec);
     if (ce != cudaSuccess) return cuda_fail(ce, "msolve loop");
 
     MSState hs;

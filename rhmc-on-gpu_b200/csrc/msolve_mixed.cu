@@ -323,28 +323,45 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     for (int j = 0; j < NR; j++) s2.alphas[j] = (Rs)coef[j];
     s2.partials = pt; s2.ticket = tk + 1; s2.fin.st = st; s2.stop = &st->stop;
 
-    cudaGraph_t graph;
-    cudaGraphExec_t exec;
-    CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-    rb_accum_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (E *)xs, st);
-    constexpr int B64 = DslashCfg<L64_18, NR, false>::block, BS1 = DslashCfg<LF, NR, false>::block,
-                  BS2 = DslashCfg<LF, NR, true>::block;
-    const int g64 = grid_for(Vh, B64), gs1 = grid_for(Vh, BS1), gs2 = grid_for(Vh, BS2);
-    dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d1);
-    dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d2);
-    rb_resid_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, bg, xg, (const double2 *)t64, (E *)rs, (E *)p, co,
-                                                         pt, tk, st);
-    for (int it = 0; it < n_ru; it++) {
-        dslash_kernel<LF, NR, false, false, NoFin><<<gs1, BS1, 0, s_>>>(s1);
-        dslash_kernel<LF, NR, true, true, FinRBAlpha<NR>><<<gs2, BS2, 0, s_>>>(s2);
-        rb_xr_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)xs, (E *)rs, (const E *)p, (const E *)ap, pt, tk + 2, st);
-        rb_p_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)rs, (E *)p, st);
+    struct Key {
+        int kind, link_reals, link_bytes, nr, n_ru, vh;
+        const void *links, *links64, *xs, *rs, *p, *ap, *h, *h64, *t64, *st, *pt, *tk, *xg, *bg;
+        double coef[RB_MAX];
+        cudaStream_t stream;
+    } key;
+    memset(&key, 0, sizeof(key));
+    key.kind = 2; key.link_reals = LF::reals; key.link_bytes = (int)sizeof(typename LF::real); key.nr = NR;
+    key.n_ru = n_ru; key.vh = Vh; key.links = lf.p; key.links64 = l64.p; key.xs = xs; key.rs = rs; key.p = p;
+    key.ap = ap; key.h = h; key.h64 = h64; key.t64 = t64; key.st = st; key.pt = pt; key.tk = tk; key.xg = xg;
+    key.bg = bg; key.stream = s_;
+    for (int j = 0; j < NR; j++) key.coef[j] = coef[j];
+    const std::string kb = key_bytes(key);
+    cudaGraphExec_t exec = c->graphs.find(kb);
+    cudaError_t ce = cudaSuccess;
+    if (!exec) {
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        rb_accum_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (E *)xs, st);
+        constexpr int B64 = DslashCfg<L64_18, NR, false>::block, BS1 = DslashCfg<LF, NR, false>::block,
+                      BS2 = DslashCfg<LF, NR, true>::block;
+        const int g64 = grid_for(Vh, B64), gs1 = grid_for(Vh, BS1), gs2 = grid_for(Vh, BS2);
+        dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d1);
+        dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d2);
+        rb_resid_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, bg, xg, (const double2 *)t64, (E *)rs, (E *)p, co,
+                                                             pt, tk, st);
+        for (int it = 0; it < n_ru; it++) {
+            dslash_kernel<LF, NR, false, false, NoFin><<<gs1, BS1, 0, s_>>>(s1);
+            dslash_kernel<LF, NR, true, true, FinRBAlpha<NR>><<<gs2, BS2, 0, s_>>>(s2);
+            rb_xr_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)xs, (E *)rs, (const E *)p, (const E *)ap, pt, tk + 2, st);
+            rb_p_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)rs, (E *)p, st);
+        }
+        ce = cudaStreamEndCapture(s_, &graph);
+        if (ce != cudaSuccess) return cuda_fail(ce, "refine capture");
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return cuda_fail(ce, "refine instantiate");
+        c->graphs.put(kb, exec);
     }
-    cudaError_t ce = cudaStreamEndCapture(s_, &graph);
-    if (ce != cudaSuccess) return cuda_fail(ce, "refine capture");
-    ce = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ce != cudaSuccess) return cuda_fail(ce, "refine instantiate");
 
     int *hflag = c->hflags;
     cudaEvent_t ev[2];
@@ -378,7 +395,6 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     c->launches += rep * (4 + 4 * (long)n_ru);
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
-    cudaGraphExecDestroy(exec);
     if (ce != cudaSuccess) return cuda_fail(ce, "refine loop");
     RBState hs;
     CK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
