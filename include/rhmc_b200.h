@@ -44,7 +44,11 @@ enum {
     RHMC_LINKS_F64_18 = 0, /* FP64, all 18 reals */
     RHMC_LINKS_F64_12 = 1, /* FP64, rows 0-1; row 2 = eta*conj(row0 x row1) (lib/Cuda/cuda_rhmc.cuh:32-45) */
     RHMC_LINKS_F32_18 = 2, /* FP32, all 18 reals */
-    RHMC_LINKS_F32_12 = 3  /* FP32, rows 0-1, reconstructed */
+    RHMC_LINKS_F32_12 = 3, /* FP32, rows 0-1, reconstructed */
+    RHMC_LINKS_F16_12 = 4  /* half precision rows 0-1, reconstructed in FP32; spinors of this format are
+                              half precision scaled per site, one 16-byte vector per site: three __half2
+                              (the colour components divided by the site's largest |re|,|im|) and that
+                              scale as a float (internal stride Vh vectors) */
 };
 
 enum { RHMC_HOST = 0, RHMC_DEVICE = 1 };
@@ -133,7 +137,9 @@ typedef struct {
     int max_iter;          /* iteration cap (max_cg, parameters.h:57) */
     int mode;              /* RHMC_MSOLVE_* */
     int fmt;               /* link format of the multi-shift phase (FP64 ones for RHMC_MSOLVE_FP64,
-                              FP32 ones for RHMC_MSOLVE_FP32, any for RHMC_MSOLVE_MIXED) */
+                              FP32 ones for RHMC_MSOLVE_FP32, any for RHMC_MSOLVE_MIXED; in mixed mode
+                              RHMC_LINKS_F16_12 means an FP32 12-real multi-shift phase followed by a
+                              refinement whose sloppy CG runs on half links and half spinors) */
     double tol_phase_a;    /* mixed mode: relative residual of the FP32 multi-shift phase (0: 3e-6) */
     double ru_delta;       /* mixed mode: FP32 residual reduction between FP64 updates (0: 0.05) */
     int certify;           /* FP64 mode: afterwards refine, by FP64 CG one system at a time, every system

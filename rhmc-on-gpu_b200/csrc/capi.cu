@@ -66,9 +66,9 @@ int rhmc_create(const rhmc_params *p, rhmc_ctx **out)
     c->device = p->device;
     c->mass = p->mass;
     c->beta = p->beta;
-    c->U64 = nullptr; c->U64_12 = nullptr; c->U32_18 = nullptr; c->U32_12 = nullptr;
+    c->U64 = nullptr; c->U64_12 = nullptr; c->U32_18 = nullptr; c->U32_12 = nullptr; c->U16_12 = nullptr;
     c->P = nullptr; c->IP = nullptr;
-    for (int i = 0; i < 4; i++) c->derived_valid[i] = false;
+    for (int i = 0; i < 5; i++) c->derived_valid[i] = false;
     c->launches = 0;
     c->hflags = nullptr;
     c->driver = nullptr;
@@ -98,7 +98,7 @@ int rhmc_destroy(rhmc_ctx *c)
     if (!c) return RHMC_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    cudaFree(c->U64); cudaFree(c->U64_12); cudaFree(c->U32_18); cudaFree(c->U32_12);
+    cudaFree(c->U64); cudaFree(c->U64_12); cudaFree(c->U32_18); cudaFree(c->U32_12); cudaFree(c->U16_12);
     cudaFree(c->P); cudaFree(c->IP);
     c->graphs.release();
     c->ws.release();
@@ -216,22 +216,22 @@ int rhmc_get_ipdot(rhmc_ctx *c, double *p, int location) { return get_algebra(c,
 
 int rhmc_spinor_to_internal(rhmc_ctx *c, int fmt, void *internal, const double *ref, int n, int location)
 {
-    if (!c || !internal || !ref || n <= 0 || fmt < 0 || fmt > 3) return fail(RHMC_ERR_ARG, "bad argument");
+    if (!c || !internal || !ref || n <= 0 || fmt < 0 || fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad argument");
     const void *d;
     int s = stage_in(c, "stage_spinor", ref, (size_t)n * c->Vh * 6 * sizeof(double), location, &d);
     if (s) return s;
-    launch_spinor_to_internal(c, fmt_is_f64(fmt), internal, (const double *)d, n);
+    launch_spinor_to_internal(c, fmt, internal, (const double *)d, n);
     CK(cudaGetLastError());
     return RHMC_OK;
 }
 
 int rhmc_spinor_from_internal(rhmc_ctx *c, int fmt, double *ref, const void *internal, int n, int location)
 {
-    if (!c || !internal || !ref || n <= 0 || fmt < 0 || fmt > 3) return fail(RHMC_ERR_ARG, "bad argument");
+    if (!c || !internal || !ref || n <= 0 || fmt < 0 || fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad argument");
     const size_t bytes = (size_t)n * c->Vh * 6 * sizeof(double);
     void *d = ref;
     if (location == RHMC_HOST) CK(c->ws.get("stage_spinor_out", bytes, &d));
-    launch_spinor_from_internal(c, fmt_is_f64(fmt), (double *)d, internal, n);
+    launch_spinor_from_internal(c, fmt, (double *)d, internal, n);
     CK(cudaGetLastError());
     if (location == RHMC_HOST) {
         CK(cudaMemcpyAsync(ref, d, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -242,17 +242,17 @@ int rhmc_spinor_from_internal(rhmc_ctx *c, int fmt, double *ref, const void *int
 
 int rhmc_dslash(rhmc_ctx *c, int fmt, int parity_out, void *out, const void *in, int n)
 {
-    if (!c || !out || !in || n <= 0 || (parity_out != 0 && parity_out != 1) || fmt < 0 || fmt > 3)
+    if (!c || !out || !in || n <= 0 || (parity_out != 0 && parity_out != 1) || fmt < 0 || fmt > RHMC_LINKS_F16_12)
         return fail(RHMC_ERR_ARG, "bad argument");
-    cudaError_t e = launch_dslash(c, fmt, parity_out, out, in, 3 * (size_t)c->Vh, n, nullptr, 0.0, 0.5, nullptr, nullptr);
+    cudaError_t e = launch_dslash(c, fmt, parity_out, out, in, spinor_stride(fmt, c->Vh), n, nullptr, 0.0, 0.5, nullptr, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "rhmc_dslash");
     return RHMC_OK;
 }
 
 int rhmc_dslash_repeat(rhmc_ctx *c, int fmt, void *even, void *odd, int n, int repeats)
 {
-    if (!c || !even || !odd || n <= 0 || repeats < 0 || fmt < 0 || fmt > 3) return fail(RHMC_ERR_ARG, "bad argument");
-    const size_t stride = 3 * (size_t)c->Vh;
+    if (!c || !even || !odd || n <= 0 || repeats < 0 || fmt < 0 || fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad argument");
+    const size_t stride = spinor_stride(fmt, c->Vh);
     for (int r = 0; r < repeats; r++) {
         cudaError_t e = launch_dslash(c, fmt, 1, odd, even, stride, n, nullptr, 0.0, 0.5, nullptr, nullptr);
         if (e == cudaSuccess) e = launch_dslash(c, fmt, 0, even, odd, stride, n, nullptr, 0.0, 0.5, nullptr, nullptr);
@@ -271,10 +271,10 @@ int rhmc_dslash_host(rhmc_ctx *c, int parity_out, double *out, const double *in)
     CK(c->ws.get("dh_iin", bytes, &iin));
     CK(c->ws.get("dh_iout", bytes, &iout));
     CK(cudaMemcpyAsync(din, in, bytes, cudaMemcpyHostToDevice, c->stream));
-    launch_spinor_to_internal(c, true, iin, (const double *)din, 1);
+    launch_spinor_to_internal(c, RHMC_LINKS_F64_18, iin, (const double *)din, 1);
     cudaError_t e = launch_dslash(c, RHMC_LINKS_F64_18, parity_out, iout, iin, 3 * (size_t)c->Vh, 1, nullptr, 0.0, 0.5, nullptr, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "rhmc_dslash_host");
-    launch_spinor_from_internal(c, true, (double *)dout, iout, 1);
+    launch_spinor_from_internal(c, RHMC_LINKS_F64_18, (double *)dout, iout, 1);
     CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return RHMC_OK;
@@ -282,13 +282,12 @@ int rhmc_dslash_host(rhmc_ctx *c, int parity_out, double *out, const double *in)
 
 int rhmc_mdagm(rhmc_ctx *c, int fmt, void *out, const void *in, double shift, int n)
 {
-    if (!c || !out || !in || n <= 0 || fmt < 0 || fmt > 3) return fail(RHMC_ERR_ARG, "bad argument");
-    const size_t es = fmt_is_f64(fmt) ? sizeof(double2) : sizeof(float2);
+    if (!c || !out || !in || n <= 0 || fmt < 0 || fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad argument");
+    const size_t st = spinor_stride(fmt, c->Vh);
     void *h;
-    CK(c->ws.get("mdagm_h", (size_t)n * 3 * c->Vh * es, &h));
-    cudaError_t e = launch_dslash(c, fmt, 1, h, in, 3 * (size_t)c->Vh, n, nullptr, 0.0, 0.5, nullptr, nullptr);
-    if (e == cudaSuccess)
-        e = launch_dslash(c, fmt, 0, out, h, 3 * (size_t)c->Vh, n, in, c->mass * c->mass + shift, -0.5, nullptr, nullptr);
+    CK(c->ws.get("mdagm_h", (size_t)n * st * spinor_elem_bytes(fmt), &h));
+    cudaError_t e = launch_dslash(c, fmt, 1, h, in, st, n, nullptr, 0.0, 0.5, nullptr, nullptr);
+    if (e == cudaSuccess) e = launch_dslash(c, fmt, 0, out, h, st, n, in, c->mass * c->mass + shift, -0.5, nullptr, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "rhmc_mdagm");
     return RHMC_OK;
 }

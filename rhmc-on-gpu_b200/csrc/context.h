@@ -96,7 +96,8 @@ struct rhmc_ctx {
     double2 *U64_12;
     float4 *U32_18;
     float4 *U32_12;
-    bool derived_valid[4];
+    uint4 *U16_12;
+    bool derived_valid[5];
     // momenta and ipdot: FP64 algebra planes [mu][parity][8][Vh]
     double *P;
     double *IP;
@@ -117,6 +118,14 @@ cudaError_t links_f64_18(rhmc_ctx *c, L64_18 *lf);
 cudaError_t links_f64_12(rhmc_ctx *c, L64_12 *lf);
 cudaError_t links_f32_18(rhmc_ctx *c, L32_18 *lf);
 cudaError_t links_f32_12(rhmc_ctx *c, L32_12 *lf);
+cudaError_t links_f16_12(rhmc_ctx *c, L16_12 *lf);
+// elements between consecutive spinors of a link format's internal storage (Vh 16-byte
+// vectors for half, 3*Vh complex numbers otherwise)
+inline size_t spinor_stride(int fmt, long Vh) { return (fmt == RHMC_LINKS_F16_12 ? 1 : 3) * (size_t)Vh; }
+inline size_t spinor_elem_bytes(int fmt)
+{
+    return (fmt == RHMC_LINKS_F64_18 || fmt == RHMC_LINKS_F64_12 || fmt == RHMC_LINKS_F16_12) ? 16 : 8;
+}
 void invalidate_links(rhmc_ctx *c);
 int grid_for(long n, int block);
 void driver_free(Driver *d);

@@ -15,7 +15,7 @@ static void run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in,
                 double alpha, double beta, double *partials)
 {
     typedef typename LF::real R;
-    typedef typename SpinorT<R>::elem E;
+    typedef typename LF::store::elem E;
     DslashArgs<LF, NR> a;
     a.g = c->g;
     a.p_out = p_out;
@@ -52,8 +52,7 @@ static void run_n(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *i
     case 8: run<LF, 8>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
     default: {
         // split into supported widths
-        typedef typename LF::real R;
-        typedef typename SpinorT<R>::elem E;
+        typedef typename LF::store::elem E;
         int done = 0;
         while (done < n) {
             int m = n - done >= 8 ? 8 : (n - done >= 4 ? 4 : n - done);
@@ -76,6 +75,7 @@ cudaError_t launch_dslash(rhmc_ctx *c, int fmt, int p_out, void *out, const void
     case RHMC_LINKS_F64_12: { L64_12 lf; e = links_f64_12(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
     case RHMC_LINKS_F32_18: { L32_18 lf; e = links_f32_18(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
     case RHMC_LINKS_F32_12: { L32_12 lf; e = links_f32_12(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
+    case RHMC_LINKS_F16_12: { L16_12 lf; e = links_f16_12(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
     default: return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess) return e;

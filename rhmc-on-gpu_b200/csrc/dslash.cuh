@@ -36,7 +36,8 @@ constexpr int DSLASH_MIN_BLOCK = 128;
 template <class LF, int NR, class FIN = NoFin>
 struct DslashArgs {
     typedef typename LF::real R;
-    typedef typename SpinorT<R>::elem E;
+    typedef typename LF::store S;  // spinor storage of in, out, y
+    typedef typename S::elem E;
     Geom g;
     int p_out;
     LF links;
@@ -85,14 +86,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
             a.links.load(mu, a.p_out, k, u, eta_of(a.g, s, mu));
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                vec3<R> v = load_spinor<R>(a.in + r * a.stride, Vh, kf);
+                vec3<R> v = LF::store::template load<R>(a.in + r * a.stride, Vh, kf);
                 mv_acc(u, v, acc[r]);
             }
             const int kb = neighbour(a.g, s, mu, -1);
             a.links.load(mu, 1 - a.p_out, kb, u, eta_back(a.g, s, mu));
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                vec3<R> v = load_spinor<R>(a.in + r * a.stride, Vh, kb);
+                vec3<R> v = LF::store::template load<R>(a.in + r * a.stride, Vh, kb);
                 mdv_sub(u, v, acc[r]);
             }
         }
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
         for (int r = 0; r < NR; r++) {
             vec3<R> o;
             if (HAS_Y) {
-                vec3<R> yv = load_spinor<R>(a.y + r * a.stride, Vh, k);
+                vec3<R> yv = LF::store::template load<R>(a.y + r * a.stride, Vh, k);
                 const R al = a.use_alphas ? a.alphas[r] : a.alpha;
 #pragma unroll
                 for (int c = 0; c < 3; c++)
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
                         red[2 * r + 1] += (double)o.c[c].re * (double)o.c[c].re + (double)o.c[c].im * (double)o.c[c].im;
                 }
             }
-            store_spinor<R>(a.out + r * a.stride, Vh, k, o);
+            LF::store::template store<R>(a.out + r * a.stride, Vh, k, o);
         }
     }
     if (RED) reduce_finalize<2 * NR>(red, a.partials, a.ticket, a.fin);

@@ -12,8 +12,8 @@ void launch_gauge_from_ref(rhmc_ctx *c, const double *ref);
 void launch_gauge_to_ref(rhmc_ctx *c, double *ref);
 void launch_algebra_from_ref(rhmc_ctx *c, double *A, const double *ref, int antiherm);
 void launch_algebra_to_ref(rhmc_ctx *c, double *ref, const double *A, int antiherm);
-void launch_spinor_to_internal(rhmc_ctx *c, bool f64, void *dst, const double *src, int n);
-void launch_spinor_from_internal(rhmc_ctx *c, bool f64, double *dst, const void *src, int n);
+void launch_spinor_to_internal(rhmc_ctx *c, int fmt, void *dst, const double *src, int n);
+void launch_spinor_from_internal(rhmc_ctx *c, int fmt, double *dst, const void *src, int n);
 
 // Largest number of right-hand sides one Dslash launch carries.
 constexpr int DSLASH_MAX_NR = 8;

@@ -53,7 +53,7 @@ __global__ void gauge_to_ref_kernel(Geom g, double2 *ref, const double2 *U)
 }
 
 // master -> derived link formats
-__global__ void derive_links_kernel(Geom g, const double2 *U, double2 *U64_12, float4 *U32_18, float4 *U32_12)
+__global__ void derive_links_kernel(Geom g, const double2 *U, double2 *U64_12, float4 *U32_18, float4 *U32_12, uint4 *U16_12)
 {
     const long Vh = g.Vh;
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -78,6 +78,16 @@ __global__ void derive_links_kernel(Geom g, const double2 *U, double2 *U64_12, f
 #pragma unroll
         for (int j = 0; j < 3; j++)
             U32_12[(mp * 3 + j) * Vh + k] = make_float4((float)e[2 * j].x, (float)e[2 * j].y, (float)e[2 * j + 1].x, (float)e[2 * j + 1].y);
+    }
+    if (U16_12) {
+        unsigned w[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            const __half2 h = __floats2half2_rn((float)e[j].x, (float)e[j].y);
+            w[j] = *reinterpret_cast<const unsigned *>(&h);
+        }
+        U16_12[mp * Vh + k] = make_uint4(w[0], w[1], w[2], w[3]);
+        reinterpret_cast<uint2 *>(U16_12 + 8 * Vh)[mp * Vh + k] = make_uint2(w[4], w[5]);
     }
 }
 
@@ -151,6 +161,28 @@ __global__ void spinor_from_internal_kernel(long Vh, int n, double2 *dst, const 
     }
 }
 
+// reference layout <-> half precision with per-site scale (H16S, Vh 16-byte vectors per spinor)
+__global__ void spinor_to_half_kernel(long Vh, int n, uint4 *dst, const double2 *src)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * Vh) return;
+    const long r = i / Vh, k = i % Vh;
+    vec3<double> v;
+#pragma unroll
+    for (int c = 0; c < 3; c++) v.c[c] = mk<double>(src[i * 3 + c].x, src[i * 3 + c].y);
+    H16S::store<double>(dst + r * Vh, (int)Vh, (int)k, v);
+}
+
+__global__ void spinor_from_half_kernel(long Vh, int n, double2 *dst, const uint4 *src)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * Vh) return;
+    const long r = i / Vh, k = i % Vh;
+    const vec3<double> v = H16S::load<double>(src + r * Vh, (int)Vh, (int)k);
+#pragma unroll
+    for (int c = 0; c < 3; c++) dst[i * 3 + c] = make_double2(v.c[c].re, v.c[c].im);
+}
+
 // ------------------------------------------------------------------ host launchers
 int grid_for(long n, int block) { return (int)((n + block - 1) / block); }
 
@@ -184,18 +216,20 @@ void launch_algebra_to_ref(rhmc_ctx *c, double *ref, const double *A, int antihe
     c->launches++;
 }
 
-void launch_spinor_to_internal(rhmc_ctx *c, bool f64, void *dst, const double *src, int n)
+void launch_spinor_to_internal(rhmc_ctx *c, int fmt, void *dst, const double *src, int n)
 {
     const int grid = grid_for((long)n * c->Vh, 256);
-    if (f64) spinor_to_internal_kernel<double2><<<grid, 256, 0, c->stream>>>(c->Vh, n, (double2 *)dst, (const double2 *)src);
+    if (fmt == RHMC_LINKS_F16_12) spinor_to_half_kernel<<<grid, 256, 0, c->stream>>>(c->Vh, n, (uint4 *)dst, (const double2 *)src);
+    else if (fmt_is_f64(fmt)) spinor_to_internal_kernel<double2><<<grid, 256, 0, c->stream>>>(c->Vh, n, (double2 *)dst, (const double2 *)src);
     else spinor_to_internal_kernel<float2><<<grid, 256, 0, c->stream>>>(c->Vh, n, (float2 *)dst, (const double2 *)src);
     c->launches++;
 }
 
-void launch_spinor_from_internal(rhmc_ctx *c, bool f64, double *dst, const void *src, int n)
+void launch_spinor_from_internal(rhmc_ctx *c, int fmt, double *dst, const void *src, int n)
 {
     const int grid = grid_for((long)n * c->Vh, 256);
-    if (f64) spinor_from_internal_kernel<double2><<<grid, 256, 0, c->stream>>>(c->Vh, n, (double2 *)dst, (const double2 *)src);
+    if (fmt == RHMC_LINKS_F16_12) spinor_from_half_kernel<<<grid, 256, 0, c->stream>>>(c->Vh, n, (double2 *)dst, (const uint4 *)src);
+    else if (fmt_is_f64(fmt)) spinor_from_internal_kernel<double2><<<grid, 256, 0, c->stream>>>(c->Vh, n, (double2 *)dst, (const double2 *)src);
     else spinor_from_internal_kernel<float2><<<grid, 256, 0, c->stream>>>(c->Vh, n, (double2 *)dst, (const float2 *)src);
     c->launches++;
 }
@@ -209,10 +243,11 @@ static cudaError_t ensure_derived(rhmc_ctx *c, int fmt)
     if (fmt == RHMC_LINKS_F64_12 && !c->U64_12) e = cudaMalloc(&p, 8 * 6 * Vh * sizeof(double2)), c->U64_12 = (double2 *)p;
     if (fmt == RHMC_LINKS_F32_18 && !c->U32_18) e = cudaMalloc(&p, 8 * 4 * Vh * sizeof(float4) + 8 * Vh * sizeof(float2)), c->U32_18 = (float4 *)p;
     if (fmt == RHMC_LINKS_F32_12 && !c->U32_12) e = cudaMalloc(&p, 8 * 3 * Vh * sizeof(float4)), c->U32_12 = (float4 *)p;
+    if (fmt == RHMC_LINKS_F16_12 && !c->U16_12) e = cudaMalloc(&p, 8 * Vh * (sizeof(uint4) + sizeof(uint2))), c->U16_12 = (uint4 *)p;
     if (e != cudaSuccess) return e;
     derive_links_kernel<<<grid_for(8L * c->Vh, 256), 256, 0, c->stream>>>(
         c->g, c->U64, fmt == RHMC_LINKS_F64_12 ? c->U64_12 : nullptr, fmt == RHMC_LINKS_F32_18 ? c->U32_18 : nullptr,
-        fmt == RHMC_LINKS_F32_12 ? c->U32_12 : nullptr);
+        fmt == RHMC_LINKS_F32_12 ? c->U32_12 : nullptr, fmt == RHMC_LINKS_F16_12 ? c->U16_12 : nullptr);
     c->launches++;
     c->derived_valid[fmt] = true;
     return cudaGetLastError();
@@ -221,11 +256,13 @@ static cudaError_t ensure_derived(rhmc_ctx *c, int fmt)
 void invalidate_links(rhmc_ctx *c)
 {
     c->derived_valid[RHMC_LINKS_F64_12] = c->derived_valid[RHMC_LINKS_F32_18] = c->derived_valid[RHMC_LINKS_F32_12] = false;
+    c->derived_valid[RHMC_LINKS_F16_12] = false;
 }
 
 cudaError_t links_f64_18(rhmc_ctx *c, L64_18 *lf) { lf->p = c->U64; lf->Vh = (int)c->Vh; return cudaSuccess; }
 cudaError_t links_f64_12(rhmc_ctx *c, L64_12 *lf) { cudaError_t e = ensure_derived(c, RHMC_LINKS_F64_12); lf->p = c->U64_12; lf->Vh = (int)c->Vh; return e; }
 cudaError_t links_f32_18(rhmc_ctx *c, L32_18 *lf) { cudaError_t e = ensure_derived(c, RHMC_LINKS_F32_18); lf->p = c->U32_18; lf->Vh = (int)c->Vh; return e; }
 cudaError_t links_f32_12(rhmc_ctx *c, L32_12 *lf) { cudaError_t e = ensure_derived(c, RHMC_LINKS_F32_12); lf->p = c->U32_12; lf->Vh = (int)c->Vh; return e; }
+cudaError_t links_f16_12(rhmc_ctx *c, L16_12 *lf) { cudaError_t e = ensure_derived(c, RHMC_LINKS_F16_12); lf->p = c->U16_12; lf->Vh = (int)c->Vh; return e; }
 
 }  // namespace rhmc

@@ -14,12 +14,16 @@
 //            direction across the update diverged for kappa ~ 1e5).  A system is finished only
 //            when that FP64 true residual is <= the target.  Systems are sorted by shift and
 //            refined in batches of up to 8 that share link loads.
+// With fmt = RHMC_LINKS_F16_12 phase A runs on FP32 12-real links and phase B's sloppy CG keeps
+// its links, residual, search direction and Dslash intermediates in half precision with a
+// per-site scale (H16S; the correction accumulates in FP32), which halves its memory traffic.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "capi_util.h"
@@ -57,9 +61,9 @@ struct RBState {
     int since[RB_MAX];     // sloppy iterations since the last update
 };
 
-// x += xs (FP64 += FP32), xs = 0, for systems not yet converged
-template <int NR, typename E>
-__global__ void __launch_bounds__(VEC_BLOCK) rb_accum_kernel(int Vh, size_t stride, double2 *x, E *xs, const RBState *st)
+// x += xs (FP64 += the sloppy accumulator X), xs = 0, for systems not yet converged
+template <int NR, typename X>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_accum_kernel(int Vh, size_t stride, double2 *x, X *xs, const RBState *st)
 {
     if (*(volatile const int *)&st->stop || !*(volatile const int *)&st->any_pending) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -71,7 +75,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_accum_kernel(int Vh, size_t stri
         for (int c = 0; c < 3; c++) {
             const size_t o = j * stride + (size_t)c * Vh + k;
             double2 xv = x[o];
-            E d = xs[o];
+            X d = xs[o];
             xv.x += (double)d.x;
             xv.y += (double)d.y;
             x[o] = xv;
@@ -113,12 +117,13 @@ struct FinRU {
     }
 };
 
-// r = b - coef*x - t (FP64), rs = (float) r, |r|^2; on the first update p = rs
-template <int NR, typename E>
-__global__ void __launch_bounds__(VEC_BLOCK) rb_resid_kernel(int Vh, size_t stride, const double2 *__restrict__ b,
+// r = b - coef*x - t (FP64), rs = r in the sloppy storage S, |r|^2; the search direction is
+// restarted from it (p = rs)
+template <int NR, class S>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_resid_kernel(int Vh, size_t stride, size_t sstride, const double2 *__restrict__ b,
                                                               const double2 *__restrict__ x, const double2 *__restrict__ t,
-                                                              E *rs, E *p, ResidCoef co, double *partials,
-                                                              unsigned *ticket, RBState *st)
+                                                              typename S::elem *rs, typename S::elem *p, ResidCoef co,
+                                                              double *partials, unsigned *ticket, RBState *st)
 {
     if (*(volatile const int *)&st->stop || !*(volatile const int *)&st->any_pending) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -129,18 +134,17 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_resid_kernel(int Vh, size_t stri
 #pragma unroll
         for (int j = 0; j < NR; j++) {
             if (st->conv[j] || !st->pending[j]) continue;
+            vec3<double> r;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const size_t o = j * stride + (size_t)c * Vh + k;
                 const double2 bv = b[o], xv = x[o], tv = t[o];
                 const double re = bv.x - co.coef[j] * xv.x - tv.x, im = bv.y - co.coef[j] * xv.y - tv.y;
                 red[j] += re * re + im * im;
-                E f;
-                f.x = re;
-                f.y = im;
-                rs[o] = f;
-                p[o] = f;  // restart the search direction from the true residual
+                r.c[c] = mk<double>(re, im);
             }
+            S::template store<double>(rs + j * sstride, Vh, k, r);
+            S::template store<double>(p + j * sstride, Vh, k, r);
         }
     }
     FinRU<NR> fin{st};
@@ -184,12 +188,14 @@ struct FinRBBeta {
     }
 };
 
-// xs += alpha p ; rs -= alpha Ap ; |rs|^2
-template <int NR, typename E>
-__global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride, E *xs, E *rs,
-                                                           const E *__restrict__ p, const E *__restrict__ ap,
-                                                           double *partials, unsigned *ticket, RBState *st)
+// xs += alpha p ; rs -= alpha Ap ; |rs|^2  (p, Ap, rs in the sloppy storage S; xs of type X)
+template <int NR, class S, typename X>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride, size_t sstride, X *xs, typename S::elem *rs,
+                                                           const typename S::elem *__restrict__ p,
+                                                           const typename S::elem *__restrict__ ap, double *partials,
+                                                           unsigned *ticket, RBState *st)
 {
+    typedef typename S::real Rs;
     if (*(volatile const int *)&st->stop) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double red[NR];
@@ -199,21 +205,21 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride,
 #pragma unroll
         for (int j = 0; j < NR; j++) {
             if (st->conv[j] || st->hold[j]) continue;
-            typedef decltype(E().x) Rs;
             const Rs a = (Rs)st->alpha[j];
+            const vec3<Rs> pv = S::template load<Rs>(p + j * sstride, Vh, k), av = S::template load<Rs>(ap + j * sstride, Vh, k);
+            vec3<Rs> rv = S::template load<Rs>(rs + j * sstride, Vh, k);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const size_t o = j * stride + (size_t)c * Vh + k;
-                const E pv = p[o], av = ap[o];
-                E xv = xs[o], rv = rs[o];
-                xv.x += a * pv.x;
-                xv.y += a * pv.y;
-                rv.x -= a * av.x;
-                rv.y -= a * av.y;
+                X xv = xs[o];
+                xv.x += a * pv.c[c].re;
+                xv.y += a * pv.c[c].im;
                 xs[o] = xv;
-                rs[o] = rv;
-                red[j] += (double)rv.x * rv.x + (double)rv.y * rv.y;
+                rv.c[c].re -= a * av.c[c].re;
+                rv.c[c].im -= a * av.c[c].im;
+                red[j] += (double)rv.c[c].re * rv.c[c].re + (double)rv.c[c].im * rv.c[c].im;
             }
+            S::template store<Rs>(rs + j * sstride, Vh, k, rv);
         }
     }
     FinRBBeta<NR> fin{st};
@@ -221,27 +227,26 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride,
 }
 
 // p = rs + beta p
-template <int NR, typename E>
-__global__ void __launch_bounds__(VEC_BLOCK) rb_p_kernel(int Vh, size_t stride, const E *__restrict__ rs, E *p,
-                                                          const RBState *st)
+template <int NR, class S>
+__global__ void __launch_bounds__(VEC_BLOCK) rb_p_kernel(int Vh, size_t sstride, const typename S::elem *__restrict__ rs,
+                                                          typename S::elem *p, const RBState *st)
 {
+    typedef typename S::real Rs;
     if (*(volatile const int *)&st->stop) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= Vh) return;
 #pragma unroll
     for (int j = 0; j < NR; j++) {
         if (st->conv[j] || st->hold[j]) continue;
-        typedef decltype(E().x) Rs;
         const Rs be = (Rs)st->beta[j];
+        const vec3<Rs> rv = S::template load<Rs>(rs + j * sstride, Vh, k);
+        vec3<Rs> pv = S::template load<Rs>(p + j * sstride, Vh, k);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const size_t o = j * stride + (size_t)c * Vh + k;
-            const E rv = rs[o];
-            E pv = p[o];
-            pv.x = rv.x + be * pv.x;
-            pv.y = rv.y + be * pv.y;
-            p[o] = pv;
+            pv.c[c].re = rv.c[c].re + be * pv.c[c].re;
+            pv.c[c].im = rv.c[c].im + be * pv.c[c].im;
         }
+        S::template store<Rs>(p + j * sstride, Vh, k, pv);
     }
 }
 
@@ -263,16 +268,19 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     AuxScope aux_scope(c);
     cudaStream_t s_ = c->aux;
     const int Vh = (int)c->Vh;
-    const size_t stride = 3 * (size_t)Vh;
+    const size_t stride = 3 * (size_t)Vh;  // FP64 fields and the accumulator xs
     void *xs, *rs, *p, *ap, *h, *h64, *t64, *stv, *part, *tick;
     typedef typename LF::real Rs;
-    typedef typename SpinorT<Rs>::elem E;
-    const size_t v32 = stride * sizeof(E), v64 = stride * sizeof(double2);
-    CK(c->ws.get("rb_xs", NR * v32, &xs));
-    CK(c->ws.get("rb_rs", NR * v32, &rs));
-    CK(c->ws.get("rb_p", NR * v32, &p));
-    CK(c->ws.get("rb_ap", NR * v32, &ap));
-    CK(c->ws.get("rb_h", NR * v32, &h));
+    typedef typename LF::store S;  // sloppy storage of rs, p, ap, h
+    typedef typename S::elem E;
+    typedef typename std::conditional<std::is_same<S, F64S>::value, double2, float2>::type X;
+    const size_t sstride = (size_t)S::planes * Vh;
+    const size_t vs = sstride * sizeof(E), vx = stride * sizeof(X), v64 = stride * sizeof(double2);
+    CK(c->ws.get("rb_xs", NR * vx, &xs));
+    CK(c->ws.get("rb_rs", NR * vs, &rs));
+    CK(c->ws.get("rb_p", NR * vs, &p));
+    CK(c->ws.get("rb_ap", NR * vs, &ap));
+    CK(c->ws.get("rb_h", NR * vs, &h));
     CK(c->ws.get("rb_h64", NR * v64, &h64));
     CK(c->ws.get("rb_t64", NR * v64, &t64));
     CK(c->ws.get("rb_state", sizeof(RBState), &stv));
@@ -298,7 +306,7 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     }
     CK(cudaMemcpyAsync(st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s_));
     CK(cudaMemsetAsync(tk, 0, 4 * sizeof(unsigned), s_));
-    CK(cudaMemsetAsync(xs, 0, NR * v32, s_));
+    CK(cudaMemsetAsync(xs, 0, NR * vx, s_));
 
     ResidCoef co;
     for (int j = 0; j < 8; j++) co.coef[j] = coef[j < NR ? j : 0];
@@ -314,12 +322,12 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     // sloppy operator
     DslashArgs<LF, NR, NoFin> s1;
     memset(&s1, 0, sizeof(s1));
-    s1.g = c->g; s1.p_out = 1; s1.links = lf; s1.in = (const E *)p; s1.out = (E *)h; s1.stride = stride;
+    s1.g = c->g; s1.p_out = 1; s1.links = lf; s1.in = (const E *)p; s1.out = (E *)h; s1.stride = sstride;
     s1.beta = (Rs)0.5; s1.stop = &st->stop;
     DslashArgs<LF, NR, FinRBAlpha<NR>> s2;
     memset(&s2, 0, sizeof(s2));
     s2.g = c->g; s2.p_out = 0; s2.links = lf; s2.in = (const E *)h; s2.out = (E *)ap; s2.y = (const E *)p;
-    s2.stride = stride; s2.beta = (Rs)-0.5; s2.use_alphas = 1;
+    s2.stride = sstride; s2.beta = (Rs)-0.5; s2.use_alphas = 1;
     for (int j = 0; j < NR; j++) s2.alphas[j] = (Rs)coef[j];
     s2.partials = pt; s2.ticket = tk + 1; s2.fin.st = st; s2.stop = &st->stop;
 
@@ -341,19 +349,20 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
     if (!exec) {
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-        rb_accum_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (E *)xs, st);
+        rb_accum_kernel<NR, X><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (X *)xs, st);
         constexpr int B64 = DslashCfg<L64_18, NR, false>::block, BS1 = DslashCfg<LF, NR, false>::block,
                       BS2 = DslashCfg<LF, NR, true>::block;
         const int g64 = grid_for(Vh, B64), gs1 = grid_for(Vh, BS1), gs2 = grid_for(Vh, BS2);
         dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d1);
         dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d2);
-        rb_resid_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, bg, xg, (const double2 *)t64, (E *)rs, (E *)p, co,
-                                                             pt, tk, st);
+        rb_resid_kernel<NR, S><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, sstride, bg, xg, (const double2 *)t64, (E *)rs, (E *)p,
+                                                             co, pt, tk, st);
         for (int it = 0; it < n_ru; it++) {
             dslash_kernel<LF, NR, false, false, NoFin><<<gs1, BS1, 0, s_>>>(s1);
             dslash_kernel<LF, NR, true, true, FinRBAlpha<NR>><<<gs2, BS2, 0, s_>>>(s2);
-            rb_xr_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)xs, (E *)rs, (const E *)p, (const E *)ap, pt, tk + 2, st);
-            rb_p_kernel<NR, E><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)rs, (E *)p, st);
+            rb_xr_kernel<NR, S, X><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, sstride, (X *)xs, (E *)rs, (const E *)p, (const E *)ap, pt,
+                                                             tk + 2, st);
+            rb_p_kernel<NR, S><<<gv, VEC_BLOCK, 0, s_>>>(Vh, sstride, (const E *)rs, (E *)p, st);
         }
         ce = cudaStreamEndCapture(s_, &graph);
         if (ce != cudaSuccess) return cuda_fail(ce, "refine capture");
@@ -517,7 +526,8 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
         A.tgt = tgt.data();
         A.res_base = std::max(res, tolA * bmax);
         A.x = xa;
-        rc = msolve_shifted(c, fmt, A, &mi);
+        // half refinement follows an FP32 multi-shift on 12-real links
+        rc = msolve_shifted(c, fmt == RHMC_LINKS_F16_12 ? RHMC_LINKS_F32_12 : fmt, A, &mi);
         if (rc && rc != RHMC_ERR_MAXITER) return rc;
         const long n = (long)nrhs * nshift * stride;
         convert_kernel<float2><<<grid_for(n, 256), 256, 0, c->stream>>>(n, x, (const float2 *)xa);
@@ -528,8 +538,12 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
     const double t_a = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     long it_b = 0;
     int ru = 0, nsys = 0;
-    // refinement: FP32 sloppy links of the matching width
-    if (fmt == RHMC_LINKS_F32_18 || fmt == RHMC_LINKS_F64_18) {
+    // refinement: half links and spinors for F16_12, else FP32 sloppy links of the matching width
+    if (fmt == RHMC_LINKS_F16_12) {
+        L16_12 lf;
+        links_f16_12(c, &lf);
+        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX, nullptr, &nsys);
+    } else if (fmt == RHMC_LINKS_F32_18 || fmt == RHMC_LINKS_F64_18) {
         L32_18 lf;
         links_f32_18(c, &lf);
         rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX,
@@ -679,6 +693,7 @@ int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const doubl
         return msolve_fp32(c, P, (double2 *)x, (const double2 *)b, info);
     }
     if (P->mode == RHMC_MSOLVE_MIXED) {
+        if (P->fmt < 0 || P->fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad link format %d", P->fmt);
         if (P->nrhs > MS_MAX_RHS) return fail(RHMC_ERR_ARG, "mixed mode batches at most %d right-hand sides", MS_MAX_RHS);
         const int nr = P->nrhs;
         if (!(nr == 1 || nr == 2 || nr == 3 || nr == 4 || nr == 8)) return fail(RHMC_ERR_ARG, "mixed mode nrhs must be 1,2,3,4 or 8");
@@ -700,10 +715,10 @@ int rhmc_msolve_host(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const 
     CK(c->ws.get("mh_x", nx * stride * sizeof(double2), &xi));
     CK(c->ws.get("mh_tmp", (nx > nb ? nx : nb) * stride * sizeof(double2), &tmp));
     CK(cudaMemcpyAsync(tmp, b, nb * stride * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    launch_spinor_to_internal(c, true, bi, (const double *)tmp, (int)nb);
+    launch_spinor_to_internal(c, RHMC_LINKS_F64_18, bi, (const double *)tmp, (int)nb);
     int rc = rhmc_msolve(c, P, (double *)xi, (const double *)bi, info);
     if (rc) return rc;
-    launch_spinor_from_internal(c, true, (double *)tmp, xi, (int)nx);
+    launch_spinor_from_internal(c, RHMC_LINKS_F64_18, (double *)tmp, xi, (int)nx);
     CK(cudaMemcpyAsync(x, tmp, nx * stride * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return RHMC_OK;

@@ -14,6 +14,7 @@
 //                                      consecutive spinors (stride 3*Vh elements)
 //   algebra  [mu][parity][8][Vh]      reals: traceless (anti-)hermitian matrices
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -122,9 +123,16 @@ __device__ __forceinline__ void reconstruct_row2(su3m<R> &u, R eta)
     u.e[2][2] = mk<R>(eta * c.re, -eta * c.im);
 }
 
+// Spinor storage policies (defined below): every link format names the storage of the spinors
+// its Dslash reads and writes.
+struct F64S;
+struct F32S;
+struct H16S;
+
 // FP64, 18 reals: 9 double2 planes
 struct L64_18 {
     typedef double real;
+    typedef F64S store;
     static constexpr int planes = 9;
     static constexpr int reals = 18;
     static constexpr int bytes = 144;
@@ -144,6 +152,7 @@ struct L64_18 {
 // FP64, 12 reals: 6 double2 planes, row 2 reconstructed
 struct L64_12 {
     typedef double real;
+    typedef F64S store;
     static constexpr int planes = 6;
     static constexpr int reals = 12;
     static constexpr int bytes = 96;
@@ -164,6 +173,7 @@ struct L64_12 {
 // FP32, 18 reals: 4 float4 planes + 1 float2 plane (the float2 planes follow all float4 ones)
 struct L32_18 {
     typedef float real;
+    typedef F32S store;
     static constexpr int planes = 5;
     static constexpr int reals = 18;
     static constexpr int bytes = 72;
@@ -186,6 +196,7 @@ struct L32_18 {
 // FP32, 12 reals: 3 float4 planes, row 2 reconstructed
 struct L32_12 {
     typedef float real;
+    typedef F32S store;
     static constexpr int planes = 3;
     static constexpr int reals = 12;
     static constexpr int bytes = 48;
@@ -198,6 +209,35 @@ struct L32_12 {
         u.e[0][0] = mk<float>(a0.x, a0.y); u.e[0][1] = mk<float>(a0.z, a0.w);
         u.e[0][2] = mk<float>(a1.x, a1.y); u.e[1][0] = mk<float>(a1.z, a1.w);
         u.e[1][1] = mk<float>(a2.x, a2.y); u.e[1][2] = mk<float>(a2.z, a2.w);
+        reconstruct_row2<float>(u, (float)eta);
+    }
+};
+
+// Half precision, 12 reals, two loads per link: a 16-byte plane (u00 u01 u02 u10 as __half2)
+// and an 8-byte plane (u11 u12) that follows all 16-byte ones; row 2 rebuilt in FP32.  SU(3)
+// entries (times the +-1 phases) lie in [-1, 1], so no scale is stored; the spinors that go
+// with these links are half with a per-site scale (H16S).
+struct L16_12 {
+    typedef float real;
+    typedef H16S store;
+    static constexpr int planes = 2;
+    static constexpr int reals = 12;
+    static constexpr int bytes = 24;
+    const uint4 *__restrict__ p;
+    int Vh;
+    __device__ __forceinline__ static cpx<float> h2c(unsigned w)
+    {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w));
+        return mk<float>(f.x, f.y);
+    }
+    __device__ __forceinline__ void load(int mu, int par, int k, su3m<float> &u, int eta) const
+    {
+        const size_t i = (size_t)(mu * 2 + par) * Vh + k;
+        const uint4 a = __ldg(p + i);
+        const uint2 b = __ldg(reinterpret_cast<const uint2 *>(p + (size_t)8 * Vh) + i);
+        u.e[0][0] = h2c(a.x); u.e[0][1] = h2c(a.y);
+        u.e[0][2] = h2c(a.z); u.e[1][0] = h2c(a.w);
+        u.e[1][1] = h2c(b.x); u.e[1][2] = h2c(b.y);
         reconstruct_row2<float>(u, (float)eta);
     }
 };
@@ -230,6 +270,97 @@ __device__ __forceinline__ void store_spinor(typename SpinorT<R>::elem *v, int V
         v[(size_t)c * Vh + k] = a;
     }
 }
+
+// Storage policies: elem is the array element type, planes the elements per site of one
+// spinor (a spinor of parity p occupies planes * Vh elements; consecutive RHS are `stride`
+// elements apart with stride >= planes * Vh).
+struct F64S {
+    typedef double real;
+    typedef double2 elem;
+    static constexpr int planes = 3;
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int Vh, int k)
+    {
+        const vec3<double> d = load_spinor<double>(v, Vh, k);
+        vec3<R> r;
+#pragma unroll
+        for (int c = 0; c < 3; c++) r.c[c] = mk<R>((R)d.c[c].re, (R)d.c[c].im);
+        return r;
+    }
+    template <typename R>
+    __device__ __forceinline__ static void store(elem *v, int Vh, int k, const vec3<R> &r)
+    {
+        vec3<double> d;
+#pragma unroll
+        for (int c = 0; c < 3; c++) d.c[c] = mk<double>((double)r.c[c].re, (double)r.c[c].im);
+        store_spinor<double>(v, Vh, k, d);
+    }
+};
+
+struct F32S {
+    typedef float real;
+    typedef float2 elem;
+    static constexpr int planes = 3;
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int Vh, int k)
+    {
+        const vec3<float> f = load_spinor<float>(v, Vh, k);
+        vec3<R> r;
+#pragma unroll
+        for (int c = 0; c < 3; c++) r.c[c] = mk<R>((R)f.c[c].re, (R)f.c[c].im);
+        return r;
+    }
+    template <typename R>
+    __device__ __forceinline__ static void store(elem *v, int Vh, int k, const vec3<R> &r)
+    {
+        vec3<float> f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) f.c[c] = mk<float>((float)r.c[c].re, (float)r.c[c].im);
+        store_spinor<float>(v, Vh, k, f);
+    }
+};
+
+// Half precision with a per-site scale, one 16-byte vector per site: words x, y, z hold the
+// three colour components as __half2 divided by the site's largest |real or imaginary part|,
+// word w holds that scale as a float (16 bytes per site instead of 24 in FP32, and one load
+// instruction per neighbour spinor).
+struct H16S {
+    typedef float real;
+    typedef uint4 elem;
+    static constexpr int planes = 1;
+    __device__ __forceinline__ static float2 h2f(unsigned w) { return __half22float2(*reinterpret_cast<const __half2 *>(&w)); }
+    __device__ __forceinline__ static unsigned f2h(float a, float b)
+    {
+        const __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const unsigned *>(&h);
+    }
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int, int k)
+    {
+        const uint4 q = __ldg(v + k);
+        const float nrm = __uint_as_float(q.w);
+        const float2 f0 = h2f(q.x), f1 = h2f(q.y), f2 = h2f(q.z);
+        vec3<R> r;
+        r.c[0] = mk<R>((R)(f0.x * nrm), (R)(f0.y * nrm));
+        r.c[1] = mk<R>((R)(f1.x * nrm), (R)(f1.y * nrm));
+        r.c[2] = mk<R>((R)(f2.x * nrm), (R)(f2.y * nrm));
+        return r;
+    }
+    template <typename R>
+    __device__ __forceinline__ static void store(elem *v, int, int k, const vec3<R> &r)
+    {
+        float m = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) m = fmaxf(m, fmaxf(fabsf((float)r.c[c].re), fabsf((float)r.c[c].im)));
+        const float inv = m > 0.f ? 1.f / m : 0.f;
+        uint4 q;
+        q.x = f2h((float)r.c[0].re * inv, (float)r.c[0].im * inv);
+        q.y = f2h((float)r.c[1].re * inv, (float)r.c[1].im * inv);
+        q.z = f2h((float)r.c[2].re * inv, (float)r.c[2].im * inv);
+        q.w = __float_as_uint(m);
+        v[k] = q;
+    }
+};
 
 // ------------------------------------------------------------------ SU(3) x vector
 // acc += U v

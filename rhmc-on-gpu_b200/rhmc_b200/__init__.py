@@ -15,8 +15,16 @@ PKG = os.path.dirname(HERE)
 LIBPATH = os.path.join(PKG, "librhmc_b200.so")
 
 RHMC_OK = 0
-LINKS_F64_18, LINKS_F64_12, LINKS_F32_18, LINKS_F32_12 = 0, 1, 2, 3
-FMT_NAMES = {LINKS_F64_18: "f64_18", LINKS_F64_12: "f64_12", LINKS_F32_18: "f32_18", LINKS_F32_12: "f32_12"}
+LINKS_F64_18, LINKS_F64_12, LINKS_F32_18, LINKS_F32_12, LINKS_F16_12 = 0, 1, 2, 3, 4
+FMT_NAMES = {LINKS_F64_18: "f64_18", LINKS_F64_12: "f64_12", LINKS_F32_18: "f32_18", LINKS_F32_12: "f32_12",
+             LINKS_F16_12: "f16_12"}
+
+
+def spinor_floats(fmt, Vh):
+    """Size of one internal spinor of a link format in 8-byte (FP64) or 4-byte units: 6*Vh
+    doubles (FP64), 6*Vh floats (FP32) or 4*Vh floats' worth of half precision with per-site
+    scales (F16_12: one 16-byte vector of three __half2 and a float scale per site)."""
+    return 4 * Vh if fmt == LINKS_F16_12 else 6 * Vh
 HOST, DEVICE = 0, 1
 
 _lib = None

@@ -14,7 +14,7 @@ def new_ctx(dims, mass=0.1, beta=5.5, bc=0):
 def internal_buffer(ctx, fmt, n=1):
     import torch
     dt = torch.float64 if fmt in (rb.LINKS_F64_18, rb.LINKS_F64_12) else torch.float32
-    return torch.zeros(n * 6 * ctx.Vh, dtype=dt, device="cuda")
+    return torch.zeros(n * rb.spinor_floats(fmt, ctx.Vh), dtype=dt, device="cuda")
 
 
 def to_internal(ctx, fmt, x):

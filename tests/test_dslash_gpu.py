@@ -1,7 +1,8 @@
 """Geometry and Dslash on the B200 against the oracle (C restatement of
 lib/Action/fermionmatrix.cc:8-97 and lib/Main/Geometry/geometry.cc:26-161).
 
-Tolerances (relative L2 norm of the difference): FP64 links 1e-13, FP32 links 1e-6.
+Tolerances (relative L2 norm of the difference): FP64 links 1e-13, FP32 links 1e-6, half
+precision links and spinors with per-site scales 2e-3 (11-bit significands).
 """
 import numpy as np
 import pytest
@@ -13,7 +14,7 @@ from conftest import rel_err
 pytestmark = pytest.mark.gpu
 
 DIMS = [(4, 4, 4, 4), (6, 4, 4, 8), (8, 8, 8, 8), (4, 6, 2, 10)]
-TOL = {rb.LINKS_F64_18: 1e-13, rb.LINKS_F64_12: 1e-13, rb.LINKS_F32_18: 1e-6, rb.LINKS_F32_12: 1e-6}
+TOL = {rb.LINKS_F64_18: 1e-13, rb.LINKS_F64_12: 1e-13, rb.LINKS_F32_18: 1e-6, rb.LINKS_F32_12: 1e-6, rb.LINKS_F16_12: 2e-3}
 
 
 @pytest.fixture(scope="module")
@@ -35,7 +36,7 @@ def test_geometry_bit_exact(dims, bc, oracle_mod):
 
 
 @pytest.mark.parametrize("dims", DIMS)
-@pytest.mark.parametrize("fmt", [rb.LINKS_F64_18, rb.LINKS_F64_12, rb.LINKS_F32_18, rb.LINKS_F32_12])
+@pytest.mark.parametrize("fmt", [rb.LINKS_F64_18, rb.LINKS_F64_12, rb.LINKS_F32_18, rb.LINKS_F32_12, rb.LINKS_F16_12])
 def test_dslash_vs_oracle(dims, fmt, oracle_mod):
     from gpu_util import new_ctx, to_internal, from_internal, internal_buffer
     ctx = new_ctx(dims)
@@ -52,7 +53,7 @@ def test_dslash_vs_oracle(dims, fmt, oracle_mod):
         assert rel_err(got, ref) < TOL[fmt], (parity, rel_err(got, ref))
 
 
-@pytest.mark.parametrize("fmt", [rb.LINKS_F64_18, rb.LINKS_F32_12])
+@pytest.mark.parametrize("fmt", [rb.LINKS_F64_18, rb.LINKS_F32_12, rb.LINKS_F16_12])
 @pytest.mark.parametrize("n", [2, 3, 4, 5, 8])
 def test_dslash_multi_rhs_matches_single(fmt, n):
     from gpu_util import new_ctx, to_internal, from_internal, internal_buffer
@@ -132,3 +133,15 @@ def test_antihermiticity_identity():
     lhs = np.vdot(ye, from_internal(ctx, fmt, a))
     rhs = -np.vdot(from_internal(ctx, fmt, b), xo)
     assert abs(lhs - rhs) < 1e-10 * abs(lhs)
+
+
+def test_half_spinor_roundtrip():
+    """Half precision with a per-site scale keeps every site to 2^-11 of its largest component."""
+    from gpu_util import new_ctx, to_internal, from_internal
+    dims = (6, 4, 4, 8)
+    ctx = new_ctx(dims)
+    x = F.random_spinor(dims, seed=9) * np.geomspace(1e-6, 1e3, ctx.Vh)[:, None]  # per-site scales over 9 decades
+    back = from_internal(ctx, rb.LINKS_F16_12, to_internal(ctx, rb.LINKS_F16_12, x))
+    site_max = np.maximum(np.abs(x.real), np.abs(x.imag)).max(1)
+    err = np.maximum(np.abs((back - x).real), np.abs((back - x).imag)).max(1)
+    assert np.all(err <= site_max * 2.0 ** -11 * 1.01)
