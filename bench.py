@@ -29,8 +29,8 @@ DIMS = (32, 32, 32, 32)
 METRIC = "multi-shift CG s/solve @1e-10 & Dslash GB/s at 32^4: mixed+batched vs plain FP64"
 
 # algorithmic bytes per output site of one half-Dslash: 8 links + 1 input + 1 output spinor
-LINK_BYTES = {0: 144, 1: 96, 2: 72, 3: 48}
-SPINOR_BYTES = {0: 48, 1: 48, 2: 24, 3: 24}
+LINK_BYTES = {0: 144, 1: 96, 2: 72, 3: 48, 4: 24}
+SPINOR_BYTES = {0: 48, 1: 48, 2: 24, 3: 24, 4: 16}  # 4: half with a per-site scale (16-byte vector)
 FLOPS_PER_SITE = 570
 
 
@@ -659,11 +659,11 @@ def main():
         return RP.max_over_ranks(v, dist, dev)
 
     results = {}
-    for fmt in (rb.LINKS_F64_18, rb.LINKS_F64_12, rb.LINKS_F32_18, rb.LINKS_F32_12):
+    for fmt in (rb.LINKS_F64_18, rb.LINKS_F64_12, rb.LINKS_F32_18, rb.LINKS_F32_12, rb.LINKS_F16_12):
         f64 = fmt in (rb.LINKS_F64_18, rb.LINKS_F64_12)
         dt = torch.float64 if f64 else torch.float32
-        xe = torch.zeros(6 * Vh, dtype=dt, device=dev)
-        xo = torch.zeros(6 * Vh, dtype=dt, device=dev)
+        xe = torch.zeros(rb.spinor_floats(fmt, Vh), dtype=dt, device=dev)
+        xo = torch.zeros(rb.spinor_floats(fmt, Vh), dtype=dt, device=dev)
         ctx.spinor_to_internal(fmt, xe, x)
         with torch.cuda.stream(stream):
             for _ in range(a.warmup):
