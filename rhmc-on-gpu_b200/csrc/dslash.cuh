@@ -10,22 +10,23 @@
 // Epilogue: out = alpha*y + beta*(2 D in)/2, i.e. beta = +0.5 gives D, beta = -0.5 with
 // alpha = mass^2 + sigma and y = p gives the even-even (M^dag M + sigma) p from D_oe p
 // (lib/Action/Inverter/inverter.cc:206-216).  With RED the kernel also reduces, per RHS,
-// Re<y, out> and |out|^2 in FP64 into per-block partials (summed by the caller's
-// last-block step, so the order of summation is fixed and results are reproducible).
+// Re<y, out> in FP64 (the <p, A p> of CG) through reduce_finalize, whose fixed summation order
+// makes results reproducible.
 #pragma once
 #include "rhmc_core.cuh"
 
 namespace rhmc {
 
 // Threads per block and the minimum resident blocks per SM handed to the register allocator,
-// per link precision, RHS count and epilogue (RED: the solver's fused reductions).  A thread
+// per link precision, RHS count and epilogue (RED: the solver's fused reductions, which need
+// blocks of 128 or 256 threads).  A thread
 // carries NR accumulators and NR neighbour spinors, so wide FP64 batches need many registers;
 // the pair trades registers (spills) against resident warps (latency hiding).  The values are
 // the fastest of the sweep in tune/dslash_tune.cu on B200 at 24^3x32 and 32^4.
 template <class LF, int NR, bool RED>
 struct DslashCfg {
     static constexpr bool f64 = sizeof(typename LF::real) == 8;
-    static constexpr bool narrow = f64 && (NR == 3 || (NR == 4 && !RED) || NR >= 8);
+    static constexpr bool narrow = f64 && NR >= 3;
     static constexpr int block = narrow ? 128 : 256;
     static constexpr int minb = (f64 && NR >= 8) ? 2 : (narrow ? 3 : 2);
 };
@@ -48,7 +49,7 @@ struct DslashArgs {
     R alpha, beta;
     R alphas[NR];       // per-RHS alpha when use_alphas (shifted systems batched together)
     int use_alphas;
-    double *partials;   // [gridDim.x][2*NR] when RED
+    double *partials;   // red_chunks(Vh) * NR doubles when RED
     unsigned *ticket;   // last-block counter when RED (fin() runs on the totals)
     FIN fin;
     const int *stop;    // optional: skip the launch when *stop != 0 ...
@@ -68,9 +69,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
     if (a.run_if && *(volatile const int *)a.run_if == 0) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int Vh = a.g.Vh;
-    double red[2 * NR > 0 ? 2 * NR : 1];
+    double red[NR];
 #pragma unroll
-    for (int j = 0; j < 2 * NR; j++) red[j] = 0.0;
+    for (int j = 0; j < NR; j++) red[j] = 0.0;
 
     if (k < Vh) {
         const Site s = site_of(a.g, a.p_out, k);
@@ -109,24 +110,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
                                    al * yv.c[c].im + a.beta * acc[r].c[c].im);
                 if (RED) {
 #pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        red[2 * r] += (double)yv.c[c].re * (double)o.c[c].re + (double)yv.c[c].im * (double)o.c[c].im;
-                        red[2 * r + 1] += (double)o.c[c].re * (double)o.c[c].re + (double)o.c[c].im * (double)o.c[c].im;
-                    }
+                    for (int c = 0; c < 3; c++)
+                        red[r] += (double)yv.c[c].re * (double)o.c[c].re + (double)yv.c[c].im * (double)o.c[c].im;
                 }
             } else {
 #pragma unroll
                 for (int c = 0; c < 3; c++) o.c[c] = mk<R>(a.beta * acc[r].c[c].re, a.beta * acc[r].c[c].im);
-                if (RED) {
-#pragma unroll
-                    for (int c = 0; c < 3; c++)
-                        red[2 * r + 1] += (double)o.c[c].re * (double)o.c[c].re + (double)o.c[c].im * (double)o.c[c].im;
-                }
             }
             LF::store::template store<R>(a.out + r * a.stride, Vh, k, o);
         }
     }
-    if (RED) reduce_finalize<2 * NR>(red, a.partials, a.ticket, a.fin);
+    if (RED) reduce_finalize<NR>(red, a.partials, a.ticket, a.fin);
 }
 
 }  // namespace rhmc

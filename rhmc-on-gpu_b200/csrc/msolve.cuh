@@ -104,7 +104,7 @@ struct FinAlpha {
             q.running = q.running_next;
             if (!q.running) continue;
             for (int i = 0; i < st->nshift; i++) q.active[i] = q.active_next[i];
-            q.alpha = tot[2 * r];
+            q.alpha = tot[r];
             if (!isfinite(q.alpha) || q.alpha == 0.0) {
                 st->status = 2;
                 st->stop = 1;

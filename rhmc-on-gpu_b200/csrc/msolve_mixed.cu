@@ -157,7 +157,7 @@ struct FinRBAlpha {
     __device__ void operator()(const double *tot) const
     {
         for (int j = 0; j < NR; j++) {
-            const double pap = tot[2 * j];
+            const double pap = tot[j];
             st->hold[j] = st->pending[j];
             const int skip = st->conv[j] || st->hold[j];
             st->alpha[j] = (skip || !(pap > 0.0)) ? 0.0 : st->rr[j] / pap;

@@ -421,19 +421,22 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double *smem)
 }
 
 // Grid-wide deterministic reduction whose result does not depend on the launch's block size.
-// Sites are summed in fixed chunks of RED_CHUNK = 128 consecutive threads (4 warps): a warp
-// shuffle tree per warp, then the 4 warp sums in order.  Every block writes one partial per
-// chunk it covers (blockDim must be a multiple of 128); the last block to finish (atomic
-// ticket) sums the chunk partials with its first 128 threads (thread t takes chunks t, t+128,
-// ... in order), then a shuffle tree per warp and the 4 warp sums in order, hands the totals to
-// fin() in thread 0 and re-arms the ticket.  A batched launch (NR right-hand sides, 128-thread
-// blocks) therefore reduces each RHS bit for bit as a single-RHS launch (256-thread blocks) does.
+// Sites are summed in fixed chunks of RED_CHUNK = 128 consecutive threads: every thread parks
+// its N values in shared memory; value j of a chunk is reduced by one warp, lane l adding
+// threads l, l+32, l+64, l+96 in that order before a shuffle tree (one shuffle tree per value
+// and chunk instead of one per value and warp).  Every block writes one partial per chunk it
+// covers (blockDim must be 128 or 256); the last block to finish (atomic ticket) sums the chunk
+// partials with its first 128 threads (thread t takes chunks t, t+128, ... in order), then a
+// shuffle tree per warp and the 4 warp sums in order, hands the totals to fin() in thread 0 and
+// re-arms the ticket.  A batched launch (NR right-hand sides, 128-thread blocks) therefore
+// reduces each RHS bit for bit as a single-RHS launch (256-thread blocks) does.
 // All threads of every block must call it.  partials: red_chunks(n) * N doubles.
 struct NoFin {
     __device__ void operator()(const double *) const {}
 };
 
 constexpr int RED_CHUNK = 128;
+constexpr int RED_BLOCK_MAX = 256;
 
 // number of chunk partials a reduction over n threads may write, for blocks of 128 or 256
 __host__ __device__ __forceinline__ long red_chunks(long n) { return 2 * ((n + 255) / 256); }
@@ -441,27 +444,24 @@ __host__ __device__ __forceinline__ long red_chunks(long n) { return 2 * ((n + 2
 template <int N, class FIN>
 __device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials, unsigned *ticket, const FIN &fin)
 {
-    __shared__ double smem[N * 32];
+    __shared__ double sm[N][RED_BLOCK_MAX];
     __shared__ int am_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int cpb = blockDim.x / RED_CHUNK;
 #pragma unroll
-    for (int j = 0; j < N; j++) v[j] = warp_sum(v[j]);
-    if (lane == 0)
-#pragma unroll
-        for (int j = 0; j < N; j++) smem[j * 32 + wid] = v[j];
+    for (int j = 0; j < N; j++) sm[j][threadIdx.x] = v[j];
     __syncthreads();
-    if (threadIdx.x < cpb) {
-        const int c = threadIdx.x;
-#pragma unroll
-        for (int j = 0; j < N; j++) {
-            double t = smem[j * 32 + 4 * c];
-            t += smem[j * 32 + 4 * c + 1];
-            t += smem[j * 32 + 4 * c + 2];
-            t += smem[j * 32 + 4 * c + 3];
-            partials[((size_t)blockIdx.x * cpb + c) * N + j] = t;
+    {
+        const int c = wid >> 2, wl = wid & 3, base = c * RED_CHUNK;
+        for (int j = wl; j < N; j += 4) {
+            double t = sm[j][base + lane];
+            t += sm[j][base + lane + 32];
+            t += sm[j][base + lane + 64];
+            t += sm[j][base + lane + 96];
+            t = warp_sum(t);
+            if (lane == 0) partials[((size_t)blockIdx.x * cpb + c) * N + j] = t;
         }
-        __threadfence();
+        if (lane == 0 && wl < N) __threadfence();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -497,16 +497,16 @@ __device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials
     for (int j = 0; j < N; j++) acc[j] = warp_sum(acc[j]);
     if (lane == 0 && wid < 4)
 #pragma unroll
-        for (int j = 0; j < N; j++) smem[j * 32 + wid] = acc[j];
+        for (int j = 0; j < N; j++) sm[j][wid] = acc[j];
     __syncthreads();
     if (threadIdx.x == 0) {
         double tot[N];
 #pragma unroll
         for (int j = 0; j < N; j++) {
-            double t = smem[j * 32];
-            t += smem[j * 32 + 1];
-            t += smem[j * 32 + 2];
-            t += smem[j * 32 + 3];
+            double t = sm[j][0];
+            t += sm[j][1];
+            t += sm[j][2];
+            t += sm[j][3];
             tot[j] = t;
         }
         *ticket = 0;
