@@ -20,6 +20,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -53,11 +54,15 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % index)
+        # the raw samples go to RHMC_CLOCKS_CSV when set (kept for inspection), else a temporary file
+        self.path = os.environ.get("RHMC_CLOCKS_CSV") or os.path.join(
+            tempfile.gettempdir(), "rhmc_clocks_%d_%d.csv" % (os.getpid(), index))
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            d = os.path.dirname(self.path)
+            if d:
+                os.makedirs(d, exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),

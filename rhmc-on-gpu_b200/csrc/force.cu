@@ -100,15 +100,17 @@ __device__ M3 staple_sum(const Geom &g, const double2 *__restrict__ U, int mu, i
 }
 
 // mode 0: ipdot = TA(U beta/3 S); mode 1: ipdot += TA(U beta/3 S).
-// One thread per site of both parities, blockIdx.y = mu: a warp covers 32 consecutive sites of
-// one parity, so every link-plane load of the warp is one contiguous 512-byte segment (own
-// links) or nearly so (neighbour links).  At 3 resident blocks per SM the register budget is
-// 170 per thread with no spills.
+// One thread per site of both parities for one mu: a warp covers 32 consecutive sites of one
+// parity, so every link-plane load of the warp is one contiguous 512-byte segment (own links)
+// or nearly so (neighbour links).  mu is the fastest-varying block index, so the four blocks of
+// a site range run together and share their links through L2 (with mu as the slow index the
+// whole link field was streamed from HBM once per mu).  At 3 resident blocks per SM the
+// register budget is 170 per thread with no spills.
 __global__ void __launch_bounds__(FORCE_BLOCK, 3) gauge_force_kernel(Geom g, const double2 *__restrict__ U, double *IP,
                                                                       double beta_by_three, int mode)
 {
-    const int mu = blockIdx.y;
-    const long site = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int mu = blockIdx.x & 3;
+    const long site = (long)(blockIdx.x >> 2) * blockDim.x + threadIdx.x;
     const int Vh = g.Vh;
     if (site >= 2L * Vh) return;
     const int p = site >= Vh;
@@ -180,8 +182,8 @@ __global__ void __launch_bounds__(FORCE_BLOCK) fermion_force_kernel(Geom g, cons
 
 int gauge_force(rhmc_ctx *c, int mode)
 {
-    const dim3 grid((unsigned)grid_for(2L * c->Vh, FORCE_BLOCK), 4);
-    gauge_force_kernel<<<grid, FORCE_BLOCK, 0, c->stream>>>(c->g, c->U64, c->IP, c->beta / 3.0, mode);
+    const long grid = 4L * grid_for(2L * c->Vh, FORCE_BLOCK);
+    gauge_force_kernel<<<(unsigned)grid, FORCE_BLOCK, 0, c->stream>>>(c->g, c->U64, c->IP, c->beta / 3.0, mode);
     c->launches++;
     CK(cudaGetLastError());
     return RHMC_OK;

@@ -2,7 +2,7 @@
 lib/Action/Inverter/inverter.cc:142-339) and against the reference's own CPU code.
 
 Tolerances: FP64 mode reproduces the reference iteration (same recurrences, FP64, FMA
-rounding only), so solutions agree to 1e-10 relative at residual 1e-10; mixed mode is judged
+rounding only), so solutions agree to 1e-10 relative at residual 1e-10; mixed mode is checked
 by the FP64 true residual of every system, which must be <= the requested residual.
 """
 import numpy as np
