@@ -145,6 +145,9 @@ typedef struct {
     int certify;           /* FP64 mode: afterwards refine, by FP64 CG one system at a time, every system
                               whose FP64 true residual is still above `residual` (the reference's
                               iterated-residual test alone can stop above it) */
+    const double *rhs_shifts; /* optional [nrhs][nshift]: a pole set per right-hand side (overrides
+                              shifts), e.g. the pseudofermions of several fermion species solved in
+                              one batch; NULL: `shifts` for every right-hand side */
 } rhmc_msolve_params;
 
 typedef struct {

@@ -133,6 +133,78 @@ static int solve(rhmc_ctx *c, int s, const Approx &ap, double res, int mode, int
     return rhmc_msolve(c, &mp, (double *)x, (const double *)b, nullptr);
 }
 
+// Every pseudofermion of every species solved against its pole set: (M^dag M(m_s) + b_{s,i}) x =
+// in_s, with in_s the species field fname(in_base, s).  When all species have the same number of
+// poles (and the batch is one the solver takes) they go through a single batched multi-shift
+// call with a pole set per right-hand side, so every link load serves all of them and a lighter
+// species' iterations carry the heavier one's at little extra cost; otherwise species by
+// species.  x ("drv_x"): species s's [no_ps][order] solutions start at spinor xoff[s].
+struct Solved {
+    std::vector<Approx> ap;   // rescaled approximation per species
+    std::vector<size_t> xoff; // first spinor of each species in x
+    double2 *x = nullptr;
+};
+
+static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res, int mode, int fmt, Solved &out)
+{
+    Driver *d = drv(c);
+    const int ns = nspecies(c);
+    out.ap.clear();
+    out.xoff.clear();
+    int total = 0;
+    bool same = true;
+    size_t xtot = 0;
+    for (int s = 0; s < ns; s++) {
+        out.ap.push_back(rescaled(c, s, which));
+        same = same && out.ap[s].order == out.ap[0].order;
+        out.xoff.push_back(xtot);
+        xtot += (size_t)d->sp[s].no_ps * out.ap[s].order;
+        total += d->sp[s].no_ps;
+    }
+    int rc = field(c, "drv_x", xtot, &out.x);
+    if (rc) return rc;
+    const bool nr_ok = mode != RHMC_MSOLVE_MIXED || total == 1 || total == 2 || total == 3 || total == 4 || total == 8;
+    if (ns == 1 || !same || total > 8 || !nr_ok) {
+        for (int s = 0; s < ns; s++) {
+            double2 *in = nullptr;
+            rc = field(c, fname(in_base, s), d->sp[s].no_ps, &in);
+            if (rc) return rc;
+            rc = solve(c, s, out.ap[s], res, mode, fmt, in, out.x + out.xoff[s] * SP(c));
+            if (rc) return rc;
+        }
+        return RHMC_OK;
+    }
+    const int order = out.ap[0].order;
+    double2 *bcat = nullptr;
+    rc = field(c, "drv_bcat", total, &bcat);
+    if (rc) return rc;
+    std::vector<double> sh((size_t)total * order);
+    int r = 0;
+    for (int s = 0; s < ns; s++) {
+        const int nps = d->sp[s].no_ps;
+        double2 *in = nullptr;
+        rc = field(c, fname(in_base, s), nps, &in);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(bcat + (size_t)r * SP(c), in, (size_t)nps * SP(c) * sizeof(double2), cudaMemcpyDeviceToDevice,
+                           c->stream));
+        const double dm2 = s == 0 ? 0.0 : d->sp[s].mass * d->sp[s].mass - c->mass * c->mass;
+        for (int ps = 0; ps < nps; ps++, r++)
+            for (int i = 0; i < order; i++) sh[(size_t)r * order + i] = out.ap[s].b[i] + dm2;
+    }
+    rhmc_msolve_params mp;
+    memset(&mp, 0, sizeof(mp));
+    mp.nshift = order;
+    mp.shifts = sh.data();
+    mp.rhs_shifts = sh.data();
+    mp.nrhs = total;
+    mp.residual = res;
+    mp.max_iter = d->P.max_cg;
+    mp.mode = mode;
+    mp.fmt = fmt;
+    d->solves++;
+    return rhmc_msolve(c, &mp, (double *)out.x, (const double *)bcat, nullptr);
+}
+
 static int check_ready(rhmc_ctx *c)
 {
     Driver *d = drv(c);
@@ -154,20 +226,19 @@ static int inv_approx_calc(rhmc_ctx *c, int which, double res)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
+    Solved sv;
+    if ((rc = solve_species(c, which, which == 0 ? "drv_phi" : "drv_chi", res, d->P.metro_mode, d->P.metro_fmt, sv))) return rc;
     for (int s = 0; s < nspecies(c); s++) {
         const int nps = d->sp[s].no_ps;
-        const Approx ap = rescaled(c, s, which);
-        double2 *phi = nullptr, *chi = nullptr, *xs = nullptr;
+        const Approx &ap = sv.ap[s];
+        double2 *phi = nullptr, *chi = nullptr;
         rc = field(c, fname("drv_phi", s), nps, &phi);
         if (rc) return rc;
         rc = field(c, fname("drv_chi", s), nps, &chi);
         if (rc) return rc;
-        rc = field(c, "drv_x", (size_t)nps * ap.order, &xs);
-        if (rc) return rc;
         const double2 *in = which == 0 ? phi : chi;
         double2 *out = which == 0 ? chi : phi;
-        if ((rc = solve(c, s, ap, res, d->P.metro_mode, d->P.metro_fmt, in, xs))) return rc;
-        if ((rc = rational_sum(c, nps, ap.order, ap.a0, ap.a.data(), xs, in, out))) return rc;
+        if ((rc = rational_sum(c, nps, ap.order, ap.a0, ap.a.data(), sv.x + sv.xoff[s] * SP(c), in, out))) return rc;
     }
     return RHMC_OK;
 }
@@ -178,16 +249,12 @@ static int fermion_part(rhmc_ctx *c, int add)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
+    Solved sv;
+    if ((rc = solve_species(c, 1, "drv_chi", d->P.residue_md, d->P.md_mode, d->P.md_fmt, sv))) return rc;
     for (int s = 0; s < nspecies(c); s++) {
-        const int nps = d->sp[s].no_ps;
-        const Approx ap = rescaled(c, s, 1);
-        double2 *chi = nullptr, *xs = nullptr;
-        rc = field(c, fname("drv_chi", s), nps, &chi);
+        const Approx &ap = sv.ap[s];
+        rc = fermion_force(c, d->sp[s].no_ps, ap.order, ap.a.data(), sv.x + sv.xoff[s] * SP(c), s == 0 ? add : 1);
         if (rc) return rc;
-        rc = field(c, "drv_x", (size_t)nps * ap.order, &xs);
-        if (rc) return rc;
-        if ((rc = solve(c, s, ap, d->P.residue_md, d->P.md_mode, d->P.md_fmt, chi, xs))) return rc;
-        if ((rc = fermion_force(c, nps, ap.order, ap.a.data(), xs, s == 0 ? add : 1))) return rc;
     }
     d->force_evals++;
     return RHMC_OK;
@@ -201,16 +268,16 @@ static int fermion_action_md(rhmc_ctx *c, double *out)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
+    Solved sv;
+    if ((rc = solve_species(c, 1, "drv_chi", d->P.residue_md, d->P.md_mode, d->P.md_fmt, sv))) return rc;
     double sum = 0.0, v;
     for (int s = 0; s < nspecies(c); s++) {
         const int nps = d->sp[s].no_ps;
-        const Approx ap = rescaled(c, s, 1);
-        double2 *chi = nullptr, *xs = nullptr;
+        const Approx &ap = sv.ap[s];
+        const double2 *xs = sv.x + sv.xoff[s] * SP(c);
+        double2 *chi = nullptr;
         rc = field(c, fname("drv_chi", s), nps, &chi);
         if (rc) return rc;
-        rc = field(c, "drv_x", (size_t)nps * ap.order, &xs);
-        if (rc) return rc;
-        if ((rc = solve(c, s, ap, d->P.residue_md, d->P.md_mode, d->P.md_fmt, chi, xs))) return rc;
         for (int ps = 0; ps < nps; ps++) {
             const double2 *cp = chi + ps * SP(c);
             if ((rc = rdot(c, cp, cp, (long)SP(c), &v))) return rc;

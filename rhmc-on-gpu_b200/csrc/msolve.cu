@@ -51,10 +51,9 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     h0.max_iter = A.max_iter;
     h0.stop_on_frozen = A.stop_on_frozen;
     h0.res = A.res_base;
-    for (int i = 0; i < S; i++) {
-        h0.tgt[i] = A.tgt[i];
-        h0.shift[i] = A.shift[i] - A.base_shift;
-    }
+    for (int i = 0; i < S; i++) h0.tgt[i] = A.tgt[i];
+    for (int r = 0; r < NR; r++)
+        for (int i = 0; i < S; i++) h0.rhs[r].shift[i] = A.shift[(size_t)r * S + i] - A.base[r];
     CK(cudaMemcpyAsync(st, &h0, sizeof(MSState), cudaMemcpyHostToDevice, s_));
     CK(cudaMemsetAsync(tk, 0, 4 * sizeof(unsigned), s_));
 
@@ -84,7 +83,9 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     a2.out = (E *)s;
     a2.y = (const E *)p;
     a2.stride = stride;
-    a2.alpha = (Rv)(c->mass * c->mass + A.base_shift);
+    a2.alpha = (Rv)(c->mass * c->mass + A.base[0]);
+    a2.use_alphas = 1;  // every RHS iterates its own base operator M^dag M + base[r]
+    for (int r = 0; r < NR; r++) a2.alphas[r] = (Rv)(c->mass * c->mass + A.base[r]);
     a2.beta = (Rv)-0.5;
     a2.partials = pt;
     a2.ticket = tk + 1;
@@ -95,13 +96,14 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     struct Key {
         int kind, link_reals, link_bytes, nr, chunk, nshift, vh;
         const void *links, *r, *p, *h, *s, *ps, *xs, *pt, *tk, *st;
-        double alpha;
+        double alpha[MS_MAX_RHS];
         cudaStream_t stream;
     } key;
     memset(&key, 0, sizeof(key));
     key.kind = 1; key.link_reals = LF::reals; key.link_bytes = (int)sizeof(typename LF::real); key.nr = NR;
     key.chunk = chunk; key.nshift = S; key.vh = Vh; key.links = lf.p; key.r = r; key.p = p; key.h = h; key.s = s;
-    key.ps = ps; key.xs = xs; key.pt = pt; key.tk = tk; key.st = st; key.alpha = (double)a2.alpha; key.stream = s_;
+    key.ps = ps; key.xs = xs; key.pt = pt; key.tk = tk; key.st = st; key.stream = s_;
+    for (int r = 0; r < NR; r++) key.alpha[r] = (double)a2.alphas[r];
     const std::string kb = key_bytes(key);
     cudaError_t ce = cudaSuccess;
     cudaGraphExec_t exec = c->graphs.find(kb);
@@ -239,7 +241,7 @@ int true_residuals(rhmc_ctx *c, int nshift, const double *shifts, int nrhs, cons
         for (int j = 0; j < 8; j++) {
             const int q = j0 + (j < J ? j : 0);
             sys.rhs[j] = q / nshift;
-            sys.coef[j] = c->mass * c->mass + shifts[q % nshift];
+            sys.coef[j] = c->mass * c->mass + shifts[q];  // [nrhs][nshift], q = r * nshift + i
         }
         const double2 *xj = x + (size_t)j0 * stride;
         cudaError_t e = launch_dslash(c, RHMC_LINKS_F64_18, 1, h, xj, stride, J, nullptr, 0.0, 0.5, nullptr, nullptr);

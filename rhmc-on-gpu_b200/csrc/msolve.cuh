@@ -41,6 +41,7 @@ struct MSRhs {
     double omegas[MS_MAX_SHIFT], gammas[MS_MAX_SHIFT];
     int active[MS_MAX_SHIFT];       // shift updated in this iteration
     int active_next[MS_MAX_SHIFT];  // after the freezing test
+    double shift[MS_MAX_SHIFT];     // sigma_{r,i} - sigma_{r,0}: this RHS's poles relative to its base
 };
 
 struct MSState {
@@ -51,7 +52,6 @@ struct MSState {
     int stop_on_frozen;             // also stop when every shift is frozen
     double res;                     // base residual target: stop when sqrt(lambda) <= res
     double tgt[MS_MAX_SHIFT];       // freezing threshold for sqrt(delta zeta''^2)
-    double shift[MS_MAX_SHIFT];     // sigma_i - sigma_0
     MSRhs rhs[MS_MAX_RHS];
 };
 
@@ -118,7 +118,7 @@ struct FinAlpha {
                 if (!q.active[i]) continue;
                 const double zi = q.zeta_i[i], zii = q.zeta_ii[i];
                 const double ziii = (zi * zii * q.omega_prev) /
-                                    (q.omega * q.gamma * (zi - zii) + zi * q.omega_prev * (1.0 - st->shift[i] * q.omega));
+                                    (q.omega * q.gamma * (zi - zii) + zi * q.omega_prev * (1.0 - q.shift[i] * q.omega));
                 q.zeta_iii[i] = ziii;
                 q.omegas[i] = q.omega * ziii / zii;
             }

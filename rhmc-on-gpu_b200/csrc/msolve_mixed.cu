@@ -442,7 +442,7 @@ static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shift
     std::vector<int> order;
     for (int q = 0; q < nshift * nrhs; q++)
         if (!skip_below || skip_below[q] > res) order.push_back(q);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int bq) { return shifts[a % nshift] < shifts[bq % nshift]; });
+    std::stable_sort(order.begin(), order.end(), [&](int a, int bq) { return shifts[a] < shifts[bq]; });
     if (nsys) *nsys = (int)order.size();
     const double m2 = c->mass * c->mass;
     size_t g0 = 0;
@@ -453,7 +453,7 @@ static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shift
         double coef[RB_MAX], tgt[RB_MAX];
         for (int j = 0; j < n; j++) {
             const int q = order[g0 + j];
-            coef[j] = m2 + shifts[q % nshift];
+            coef[j] = m2 + shifts[q];  // shifts [nrhs][nshift], q = r * nshift + i
             tgt[j] = res;
             CK(cudaMemcpyAsync((double2 *)xg + j * stride, x + (size_t)q * stride, v64, cudaMemcpyDeviceToDevice, c->stream));
             CK(cudaMemcpyAsync((double2 *)bg + j * stride, b + (size_t)(q / nshift) * stride, v64, cudaMemcpyDeviceToDevice,
@@ -478,13 +478,16 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
 {
     const size_t stride = 3 * (size_t)c->Vh;
     auto t0 = std::chrono::steady_clock::now();
-    double smin = shifts[0];
-    for (int i = 1; i < nshift; i++) smin = std::min(smin, shifts[i]);
+    std::vector<double> base(nrhs);  // each RHS iterates on its smallest pole
+    for (int r = 0; r < nrhs; r++) {
+        base[r] = shifts[(size_t)r * nshift];
+        for (int i = 1; i < nshift; i++) base[r] = std::min(base[r], shifts[(size_t)r * nshift + i]);
+    }
     MSolveArgs A;
     A.nshift = nshift;
     A.nrhs = nrhs;
     A.shift = shifts;
-    A.base_shift = smin;
+    A.base = base.data();
     A.max_iter = max_iter;
     A.stop_on_frozen = 1;
     A.chunk = 8;
@@ -571,10 +574,12 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
 
 using namespace rhmc;
 
-static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, const double2 *b, rhmc_msolve_info *info)
+// sh: the pole sets [nrhs][nshift]
+static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, const double *sh, double2 *x, const double2 *b,
+                       rhmc_msolve_info *info)
 {
     const size_t stride = 3 * (size_t)c->Vh;
-    std::vector<double> tgt(P->nshift, P->residual);
+    std::vector<double> tgt(P->nshift, P->residual), zero(MS_MAX_RHS, 0.0);
     int done = 0, rc = RHMC_OK;
     auto t0 = std::chrono::steady_clock::now();
     while (done < P->nrhs) {
@@ -583,8 +588,8 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, con
         MSolveArgs A;
         A.nshift = P->nshift;
         A.nrhs = n;
-        A.shift = P->shifts;
-        A.base_shift = 0.0;
+        A.shift = sh + (size_t)done * P->nshift;
+        A.base = zero.data();  // the reference iterates on M^dag M itself
         A.tgt = tgt.data();
         A.res_base = P->residual;
         A.max_iter = P->max_iter;
@@ -607,13 +612,12 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, con
     if (rc == RHMC_OK && P->certify) {
         // FP64 defect correction of every system whose FP64 true residual is above target
         std::vector<double> tr((size_t)P->nshift * P->nrhs);
-        rc = true_residuals(c, P->nshift, P->shifts, P->nrhs, x, b, tr.data());
+        rc = true_residuals(c, P->nshift, sh, P->nrhs, x, b, tr.data());
         for (double &v : tr) v = std::sqrt(v);
         if (rc == RHMC_OK) {
             L64_18 lf;
             links_f64_18(c, &lf);
-            rc = refine_all(c, lf, P->nshift, P->shifts, P->nrhs, P->residual, P->max_iter, x, b, &it_b, &ru, 0.05, 1, tr.data(),
-                            &nsys);
+            rc = refine_all(c, lf, P->nshift, sh, P->nrhs, P->residual, P->max_iter, x, b, &it_b, &ru, 0.05, 1, tr.data(), &nsys);
         }
         cudaStreamSynchronize(c->stream);
     }
@@ -630,10 +634,11 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, con
 
 // The reference's single-precision path (cuda_shifted_inverter, lib/Cuda/cuda_inverter.cu:647-857):
 // the same recurrences with FP32 links and vectors, FP64 scalars; solutions returned in FP64.
-static int msolve_fp32(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, const double2 *b, rhmc_msolve_info *info)
+static int msolve_fp32(rhmc_ctx *c, const rhmc_msolve_params *P, const double *sh, double2 *x, const double2 *b,
+                       rhmc_msolve_info *info)
 {
     const size_t stride = 3 * (size_t)c->Vh;
-    std::vector<double> tgt(P->nshift, P->residual);
+    std::vector<double> tgt(P->nshift, P->residual), zero(MS_MAX_RHS, 0.0);
     auto t0 = std::chrono::steady_clock::now();
     int done = 0, rc = RHMC_OK;
     void *xa;
@@ -644,8 +649,8 @@ static int msolve_fp32(rhmc_ctx *c, const rhmc_msolve_params *P, double2 *x, con
         MSolveArgs A;
         A.nshift = P->nshift;
         A.nrhs = n;
-        A.shift = P->shifts;
-        A.base_shift = 0.0;
+        A.shift = sh + (size_t)done * P->nshift;
+        A.base = zero.data();
         A.tgt = tgt.data();
         A.res_base = P->residual;
         A.max_iter = P->max_iter;
@@ -677,20 +682,25 @@ extern "C" {
 
 int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const double *b, rhmc_msolve_info *info)
 {
-    if (!c || !P || !x || !b || !P->shifts) return fail(RHMC_ERR_ARG, "null argument");
+    if (!c || !P || !x || !b || (!P->shifts && !P->rhs_shifts)) return fail(RHMC_ERR_ARG, "null argument");
     if (P->nshift < 1 || P->nshift > MS_MAX_SHIFT) return fail(RHMC_ERR_ARG, "nshift must be in [1, %d]", MS_MAX_SHIFT);
     if (P->nrhs < 1) return fail(RHMC_ERR_ARG, "nrhs must be >= 1");
     if (P->max_iter < 1) return fail(RHMC_ERR_ARG, "max_iter must be >= 1");
-    for (int i = 0; i < P->nshift; i++)
-        if (!(P->shifts[i] >= 0.0)) return fail(RHMC_ERR_ARG, "shifts must be >= 0");
+    // the pole set of every RHS: rhs_shifts [nrhs][nshift], or shifts for all of them
+    std::vector<double> sh((size_t)P->nrhs * P->nshift);
+    for (int r = 0; r < P->nrhs; r++)
+        for (int i = 0; i < P->nshift; i++)
+            sh[(size_t)r * P->nshift + i] = P->rhs_shifts ? P->rhs_shifts[(size_t)r * P->nshift + i] : P->shifts[i];
+    for (double v : sh)
+        if (!(v >= 0.0)) return fail(RHMC_ERR_ARG, "shifts must be >= 0");
     if (info) memset(info, 0, sizeof(*info));
     if (P->mode == RHMC_MSOLVE_FP64) {
         if (P->fmt != RHMC_LINKS_F64_18 && P->fmt != RHMC_LINKS_F64_12) return fail(RHMC_ERR_ARG, "FP64 mode needs FP64 links");
-        return msolve_fp64(c, P, (double2 *)x, (const double2 *)b, info);
+        return msolve_fp64(c, P, sh.data(), (double2 *)x, (const double2 *)b, info);
     }
     if (P->mode == RHMC_MSOLVE_FP32) {
         if (P->fmt != RHMC_LINKS_F32_18 && P->fmt != RHMC_LINKS_F32_12) return fail(RHMC_ERR_ARG, "FP32 mode needs FP32 links");
-        return msolve_fp32(c, P, (double2 *)x, (const double2 *)b, info);
+        return msolve_fp32(c, P, sh.data(), (double2 *)x, (const double2 *)b, info);
     }
     if (P->mode == RHMC_MSOLVE_MIXED) {
         if (P->fmt < 0 || P->fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad link format %d", P->fmt);
@@ -699,7 +709,7 @@ int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const doubl
         if (!(nr == 1 || nr == 2 || nr == 3 || nr == 4 || nr == 8)) return fail(RHMC_ERR_ARG, "mixed mode nrhs must be 1,2,3,4 or 8");
         const double tolA = P->tol_phase_a > 0 ? P->tol_phase_a : 3e-6;
         const double rud = (P->ru_delta > 0 && P->ru_delta < 1) ? P->ru_delta : 0.05;
-        return msolve_mixed(c, P->fmt, P->nshift, P->shifts, nr, P->residual, P->max_iter, tolA, rud, (double2 *)x,
+        return msolve_mixed(c, P->fmt, P->nshift, sh.data(), nr, P->residual, P->max_iter, tolA, rud, (double2 *)x,
                             (const double2 *)b, info);
     }
     return fail(RHMC_ERR_ARG, "bad solver mode %d", P->mode);
@@ -727,7 +737,10 @@ int rhmc_msolve_host(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const 
 int rhmc_true_residuals(rhmc_ctx *c, int nshift, const double *shifts, int nrhs, const double *x, const double *b, double *out)
 {
     if (!c || !shifts || !x || !b || !out || nshift < 1 || nrhs < 1) return fail(RHMC_ERR_ARG, "bad argument");
-    int rc = true_residuals(c, nshift, shifts, nrhs, (const double2 *)x, (const double2 *)b, out);
+    std::vector<double> sh((size_t)nrhs * nshift);
+    for (int r = 0; r < nrhs; r++)
+        for (int i = 0; i < nshift; i++) sh[(size_t)r * nshift + i] = shifts[i];
+    int rc = true_residuals(c, nshift, sh.data(), nrhs, (const double2 *)x, (const double2 *)b, out);
     if (rc) return rc;
     for (int i = 0; i < nshift * nrhs; i++) out[i] = std::sqrt(out[i]);
     return RHMC_OK;

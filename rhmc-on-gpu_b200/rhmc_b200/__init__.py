@@ -205,7 +205,8 @@ MSOLVE_FP64, MSOLVE_MIXED, MSOLVE_FP32 = 0, 1, 2
 class MsolveParams(ctypes.Structure):
     _fields_ = [("nshift", ctypes.c_int), ("shifts", ctypes.POINTER(ctypes.c_double)), ("nrhs", ctypes.c_int),
                 ("residual", ctypes.c_double), ("max_iter", ctypes.c_int), ("mode", ctypes.c_int), ("fmt", ctypes.c_int),
-                ("tol_phase_a", ctypes.c_double), ("ru_delta", ctypes.c_double), ("certify", ctypes.c_int)]
+                ("tol_phase_a", ctypes.c_double), ("ru_delta", ctypes.c_double), ("certify", ctypes.c_int),
+                ("rhs_shifts", ctypes.POINTER(ctypes.c_double))]
 
 
 class MsolveInfo(ctypes.Structure):
@@ -220,9 +221,14 @@ class MsolveInfo(ctypes.Structure):
 
 
 def _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a=0.0, certify=0, ru_delta=0.0):
+    """shifts: one pole set (nshift,) for every RHS, or one per RHS (nrhs, nshift)."""
     sh = np.ascontiguousarray(shifts, np.float64)
-    p = MsolveParams(len(sh), sh.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nrhs, residual, max_iter, mode, fmt,
-                     tol_phase_a, ru_delta, certify)
+    per_rhs = sh.ndim == 2
+    if per_rhs:
+        assert sh.shape[0] == nrhs, "one pole set per right-hand side"
+    dp = ctypes.POINTER(ctypes.c_double)
+    p = MsolveParams(sh.shape[-1], sh.ctypes.data_as(dp), nrhs, residual, max_iter, mode, fmt, tol_phase_a, ru_delta, certify,
+                     sh.ctypes.data_as(dp) if per_rhs else None)
     p._keep = sh
     return p
 
@@ -243,7 +249,7 @@ def _ctx_msolve_host(self, b, shifts, residual, max_iter=100000, mode=MSOLVE_FP6
     b = np.ascontiguousarray(b, np.complex128)
     single = b.ndim == 2
     nrhs = 1 if single else b.shape[0]
-    x = np.zeros((nrhs, len(shifts), self.Vh, 3), np.complex128)
+    x = np.zeros((nrhs, np.shape(shifts)[-1], self.Vh, 3), np.complex128)
     p = _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a, certify)
     info = MsolveInfo()
     self.call("rhmc_msolve_host", ctypes.byref(p), x, b, ctypes.byref(info))
