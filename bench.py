@@ -505,7 +505,7 @@ def rhmc4_bench(a, rb, F, np, torch, rank, dev, stream):
     from rhmc_b200 import rational as R
     dims = (4, 4, 4, 4)
     lo, hi = 1e-3, 64.0 / 1.05  # the rescale widens the top by 1.05: range [1e-3, 64]
-    eps = lo / 64.0
+    eps = 0.95 * lo / 64.0      # ... and the bottom by 0.95 (rationalapprox.cc:147-170)
     ap_ = [R.rational_power(0.25, 8, eps), R.rational_power(-0.5, 8, eps), R.rational_power(-0.5, 8, eps)]
     ntraj = 5
     uni = np.random.Generator(np.random.Philox(4004)).random(ntraj)
