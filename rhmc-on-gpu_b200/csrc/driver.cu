@@ -135,10 +135,10 @@ static int solve(rhmc_ctx *c, int s, const Approx &ap, double res, int mode, int
 
 // Every pseudofermion of every species solved against its pole set: (M^dag M(m_s) + b_{s,i}) x =
 // in_s, with in_s the species field fname(in_base, s).  When all species have the same number of
-// poles (and the batch is one the solver takes) they go through a single batched multi-shift
-// call with a pole set per right-hand side, so every link load serves all of them and a lighter
-// species' iterations carry the heavier one's at little extra cost; otherwise species by
-// species.  x ("drv_x"): species s's [no_ps][order] solutions start at spinor xoff[s].
+// poles they go through a single batched multi-shift call with a pole set per right-hand side,
+// so every link load serves all of them and a lighter species' iterations carry the heavier
+// one's at little extra cost; otherwise species by species.  x ("drv_x"): species s's
+// [no_ps][order] solutions start at spinor xoff[s].
 struct Solved {
     std::vector<Approx> ap;   // rescaled approximation per species
     std::vector<size_t> xoff; // first spinor of each species in x
@@ -163,8 +163,7 @@ static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res
     }
     int rc = field(c, "drv_x", xtot, &out.x);
     if (rc) return rc;
-    const bool nr_ok = mode != RHMC_MSOLVE_MIXED || total == 1 || total == 2 || total == 3 || total == 4 || total == 8;
-    if (ns == 1 || !same || total > 8 || !nr_ok) {
+    if (ns == 1 || !same) {
         for (int s = 0; s < ns; s++) {
             double2 *in = nullptr;
             rc = field(c, fname(in_base, s), d->sp[s].no_ps, &in);

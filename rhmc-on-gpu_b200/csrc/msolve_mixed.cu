@@ -704,13 +704,30 @@ int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const doubl
     }
     if (P->mode == RHMC_MSOLVE_MIXED) {
         if (P->fmt < 0 || P->fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad link format %d", P->fmt);
-        if (P->nrhs > MS_MAX_RHS) return fail(RHMC_ERR_ARG, "mixed mode batches at most %d right-hand sides", MS_MAX_RHS);
-        const int nr = P->nrhs;
-        if (!(nr == 1 || nr == 2 || nr == 3 || nr == 4 || nr == 8)) return fail(RHMC_ERR_ARG, "mixed mode nrhs must be 1,2,3,4 or 8");
         const double tolA = P->tol_phase_a > 0 ? P->tol_phase_a : 3e-6;
         const double rud = (P->ru_delta > 0 && P->ru_delta < 1) ? P->ru_delta : 0.05;
-        return msolve_mixed(c, P->fmt, P->nshift, sh.data(), nr, P->residual, P->max_iter, tolA, rud, (double2 *)x,
-                            (const double2 *)b, info);
+        // batches of 8, 4, 3, 2 or 1 right-hand sides (the widths the kernels are built for)
+        const size_t stride = 3 * (size_t)c->Vh;
+        int done = 0, rc = RHMC_OK;
+        rhmc_msolve_info agg, part;
+        memset(&agg, 0, sizeof(agg));
+        while (done < P->nrhs && rc == RHMC_OK) {
+            const int left = P->nrhs - done;
+            const int n = left >= 8 ? 8 : (left >= 4 ? 4 : left);
+            memset(&part, 0, sizeof(part));
+            rc = msolve_mixed(c, P->fmt, P->nshift, sh.data() + (size_t)done * P->nshift, n, P->residual, P->max_iter, tolA, rud,
+                              (double2 *)x + (size_t)done * P->nshift * stride, (const double2 *)b + (size_t)done * stride, &part);
+            for (int j = 0; j < n && done + j < 8; j++) agg.iters[done + j] = part.iters[j];
+            agg.refine_iters += part.refine_iters;
+            agg.reliable_updates += part.reliable_updates;
+            agg.seconds += part.seconds;
+            agg.seconds_phase_a += part.seconds_phase_a;
+            agg.systems_refined += part.systems_refined;
+            done += n;
+        }
+        agg.status = rc;
+        if (info) *info = agg;
+        return rc;
     }
     return fail(RHMC_ERR_ARG, "bad solver mode %d", P->mode);
 }

@@ -77,7 +77,7 @@ def test_msolve_batched_rhs_identical():
 
 
 @pytest.mark.parametrize("fmt", [rb.LINKS_F32_12, rb.LINKS_F32_18, rb.LINKS_F16_12])
-@pytest.mark.parametrize("nrhs", [1, 4])
+@pytest.mark.parametrize("nrhs", [1, 4, 5])
 def test_msolve_mixed_true_residual(fmt, nrhs, oracle_mod):
     from gpu_util import new_ctx
     import torch
