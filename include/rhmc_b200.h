@@ -217,6 +217,11 @@ typedef struct {
     double residue_md;    /* force solves, parameters.h:73 */
     int metro_mode, metro_fmt; /* RHMC_MSOLVE_* and link format of the heatbath/action solves */
     int md_mode, md_fmt;       /* ... of the force solves */
+    int auto_bounds;      /* spectral bounds of M^dag M: 0 from rhmc_set_eig_bounds; 1 by FP64 power
+                             iterations for lambda_max and lambda_min (findminmax, findminmax.cc:12-183)
+                             at the start of every trajectory, instead of at every rescaling as the
+                             reference does; 2 lambda_max by power iteration, lambda_min = mass^2 (the
+                             exact lower bound of M^dag M, no slow lambda_min iteration) */
 } rhmc_driver_params;
 
 /* Configures the driver of lib/Update (update.cc, ipdot.cc, momenta.cc, MD_integrators).
@@ -238,6 +243,9 @@ int rhmc_set_approx(rhmc_ctx *ctx, int which, int order, double a0, const double
 /* Spectral bounds of M^dag M (at the selected species' mass) that findminmax would return (findminmax.cc:140-183); the rescaling
  * widens them by 0.95 / 1.05 like RationalApprox::*_inv_approx_coeff (rationalapprox.cc:134-266). */
 int rhmc_set_eig_bounds(rhmc_ctx *ctx, double min, double max);
+/* The bounds the driver currently holds for the selected species (set, or computed when
+ * auto_bounds is on). */
+int rhmc_get_eig_bounds(rhmc_ctx *ctx, double *min, double *max);
 /* Pseudofermions phi and chi, reference layout complex[no_ps][Vh][3] (MultiFermion). */
 int rhmc_set_phi(rhmc_ctx *ctx, const double *phi, int location);
 int rhmc_get_phi(rhmc_ctx *ctx, double *phi, int location);

@@ -28,10 +28,13 @@
 #include <string>
 #include <vector>
 
+#include <random>
+
 #include "capi_util.h"
 #include "context.h"
 #include "kernels.h"
 #include "solver.h"
+#include "../../include/rhmc_legacy.h"
 
 namespace rhmc {
 
@@ -64,6 +67,7 @@ struct Driver {
     std::vector<Species> sp;  // sp[0]: the context mass with P.no_flavours, P.no_ps
     int cur = 0;              // the species the approx / bounds / phi / chi setters act on
     long force_evals = 0, solves = 0;
+    std::vector<double> pw_start;  // start vector of the power iterations (auto_bounds)
 };
 
 static Driver *drv(rhmc_ctx *c) { return c->driver; }
@@ -204,10 +208,41 @@ static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res
     return rhmc_msolve(c, &mp, (double *)out.x, (const double *)bcat, nullptr);
 }
 
+// findminmax (findminmax.cc:140-183) on the device, for the current links: FP64 power iterations
+// for lambda_max of M^dag M at the context mass and (auto_bounds 1) for lambda_min through
+// lambda_max - M^dag M, or (auto_bounds 2) lambda_min = mass^2; a species of mass m_s gets both
+// shifted by m_s^2 - m^2.  The start vector is a fixed pseudo-random spinor.
+static int compute_bounds(rhmc_ctx *c)
+{
+    Driver *d = drv(c);
+    if (d->pw_start.size() != 6 * (size_t)c->Vh) {
+        std::mt19937_64 rng(0x5eedULL);
+        std::normal_distribution<double> nd(0.0, 1.0);
+        d->pw_start.resize(6 * (size_t)c->Vh);
+        for (double &v : d->pw_start) v = nd(rng);
+    }
+    double mx = 0.0, mn = c->mass * c->mass;
+    int rc = rhmc_find_max(c, d->pw_start.data(), &mx);
+    if (rc) return rc;
+    if (d->P.auto_bounds == 1 && (rc = rhmc_find_min(c, d->pw_start.data(), mx, &mn))) return rc;
+    for (int s = 0; s < nspecies(c); s++) {
+        Species &S = d->sp[s];
+        const double dm2 = S.mass * S.mass - c->mass * c->mass;
+        S.eig_min = mn + dm2;
+        S.eig_max = mx + dm2;
+        S.have_bounds = true;
+    }
+    return RHMC_OK;
+}
+
 static int check_ready(rhmc_ctx *c)
 {
     Driver *d = drv(c);
     if (!d || !d->configured) return fail(RHMC_ERR_STATE, "driver not configured (rhmc_driver_setup)");
+    if (d->P.auto_bounds && !d->sp[0].have_bounds) {
+        const int rc = compute_bounds(c);
+        if (rc) return rc;
+    }
     for (int s = 0; s < nspecies(c); s++) {
         const Species &S = d->sp[s];
         if (!S.have_bounds) return fail(RHMC_ERR_STATE, "species %d: eigenvalue bounds not set (rhmc_set_eig_bounds)", s);
@@ -512,6 +547,7 @@ int rhmc_driver_setup(rhmc_ctx *c, const rhmc_driver_params *p)
     if (p->no_ps < 1 || p->no_flavours < 1 || p->no_md < 1 || p->gauge_scale < 1 || p->max_cg < 1)
         return fail(RHMC_ERR_ARG, "no_ps, no_flavours, no_md, gauge_scale and max_cg must be positive");
     if (p->integrator < 0 || p->integrator > RHMC_INT_LEAPFROG) return fail(RHMC_ERR_ARG, "unknown integrator");
+    if (p->auto_bounds < 0 || p->auto_bounds > 2) return fail(RHMC_ERR_ARG, "auto_bounds must be 0, 1 or 2");
     Driver *d = ensure_driver(c);
     d->P = *p;
     d->sp[0].no_flavours = p->no_flavours;
@@ -569,6 +605,17 @@ int rhmc_set_eig_bounds(rhmc_ctx *c, double min, double max)
     return RHMC_OK;
 }
 
+int rhmc_get_eig_bounds(rhmc_ctx *c, double *min, double *max)
+{
+    if (!c || !min || !max) return fail(RHMC_ERR_ARG, "null argument");
+    if (!c->driver) return fail(RHMC_ERR_STATE, "driver not configured");
+    const Species &S = c->driver->sp[c->driver->cur];
+    if (!S.have_bounds) return fail(RHMC_ERR_STATE, "no spectral bounds yet");
+    *min = S.eig_min;
+    *max = S.eig_max;
+    return RHMC_OK;
+}
+
 // the pseudofermions of the selected species
 static int pf_io(rhmc_ctx *c, const char *name, double *host_ref, int location, int to_device)
 {
@@ -601,9 +648,10 @@ int rhmc_copy_saved(rhmc_ctx *c) { return c ? copy_saved(c) : fail(RHMC_ERR_ARG,
 int rhmc_update(rhmc_ctx *c, double uniform, int *acc, double *delta_s)
 {
     if (!c || !acc) return fail(RHMC_ERR_ARG, "null argument");
-    int rc = check_ready(c);
-    if (rc) return rc;
     Driver *d = drv(c);
+    int rc;
+    if (d && d->configured && d->P.auto_bounds && (rc = compute_bounds(c))) return rc;  // once per trajectory
+    if ((rc = check_ready(c))) return rc;
     if ((rc = save_conf(c))) return rc;
     if ((rc = inv_approx_calc(c, 0, d->P.residue_metro))) return rc;
     double s0, s1;

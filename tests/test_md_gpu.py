@@ -145,3 +145,34 @@ def test_driver_errors_and_reject_restores_links():
     de, acc = ctx2.update(float(g["uniform"]))
     assert acc == 0
     assert np.array_equal(ctx2.get_gauge(), g["u"])
+
+
+@pytest.mark.parametrize("auto", [1, 2])
+def test_driver_auto_bounds(auto):
+    """auto_bounds: the driver computes lambda_min/max of M^dag M by FP64 power iterations at the
+    start of every trajectory (as findminmax does at every rescaling); with 2 lambda_min = m^2.
+    The bounds must enclose the spectrum the power iterations of the legacy entry points give and
+    a trajectory must run with them."""
+    from gpu_util import new_ctx
+    g = load("t4")
+    mass = float(g["mass"])
+    ctx = new_ctx(tuple(g["dims"]), mass=mass, beta=float(g["beta"]))
+    ctx.set_gauge(g["u"])
+    ctx.driver_setup(no_flavours=2, no_ps=1, no_md=4, integrator=rb.INT_LEAPFROG, auto_bounds=auto)
+    for w, c in enumerate(coeffs("t4")):
+        ctx.set_approx(w, c)
+    # the bounds belong to the trajectory's starting configuration
+    ref_max = ctx.find_max(F.random_spinor(tuple(g["dims"]), seed=77))
+    ctx.set_momenta(g["P"])
+    ctx.set_phi(g["phi"])
+    de, acc = ctx.update(0.5)
+    assert np.isfinite(de)
+    mn, mx = ctx.eig_bounds()
+    # two power iterations from different starts; the 5e-4 stop on the relative change of the norm
+    # leaves each a little below lambda_max when the top eigenvalues are close (the rescaling's
+    # factor 1.05 covers that, as in the reference)
+    assert abs(mx - ref_max) <= 2e-2 * ref_max
+    if auto == 2:
+        assert mn == mass * mass
+    else:
+        assert mass * mass * 0.999 < mn < mx
