@@ -199,7 +199,7 @@ MS_DIMS = (24, 24, 24, 32)
 
 
 def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False, nrhs=4, nshift=16, res=1e-10, only=(),
-                 mass=0.01, warmup=True):
+                 mass=0.01, warmup=True, cpu=False):
     """Multi-shift CG, am=0.01: 16 poles log-spaced in [1e-4, 50], 4 Gaussian RHS, true residual
     1e-10 for every (RHS, pole) system: absolute |b - (M^dag M + s) x| <= 1e-10 (the reference's
     stopping criterion, inverter.cc:287) or, with relative, <= 1e-10 |b| (at 32^4 the absolute
@@ -268,6 +268,37 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False,
     free, total = torch.cuda.mem_get_info(dev)
     out["device_memory_in_use_gb"] = round((total - free) / 1e9, 2)  # workspaces of all variants, at the end
     ctx.close()
+    tag = {(24, 24, 24, 32): "m24", (32, 32, 32, 32): "m32"}.get(tuple(dims))
+    if cpu and tag and nshift == 16 and abs(mass - 0.01) < 1e-12:
+        out["cpu_reference"] = reference_msolve_timing(tag, u, b_host[0], shifts, np,
+                                                       out.get("fp64_single_rhs", {}).get("iters", [None])[0], nrhs)
+    return out
+
+
+def reference_msolve_timing(tag, u, b, shifts, np, iters, nrhs):
+    """The reference's own CPU multi-shift solver (multips_shifted_invert,
+    lib/Action/Inverter/inverter.cc:142-339, unmodified, behind the harness in
+    oracle/_ref/libref_<tag>.so, built with max_cg = 100 (24^3x32) or 60 (32^4)) on the same links,
+    right-hand side and poles, on one host core: seconds per iteration over its first max_cg
+    iterations (all 16 poles still active, so an upper figure for the average iteration), and
+    that figure times the B200 solve's iteration count as the estimated CPU time of the solve."""
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        ref = oracle.RefLib(tag)
+    except Exception as e:
+        return {"unavailable": str(e)[:200]}
+    ref.set_links(u)
+    ref.set_chi(np.asarray(b)[None])
+    n_it = int(ref.lib.ref_param(5))  # max_cg of the build
+    t0 = time.perf_counter()
+    ref.msolve(1e-10, shifts)
+    dt = time.perf_counter() - t0
+    out = {"kind": "reference", "cores": 1, "iterations_timed": n_it, "s_per_iteration": round(dt / n_it, 5),
+           "sample": "first %d iterations of one right-hand side, 16 poles, FP64" % n_it}
+    if iters:
+        out["est_s_per_solve"] = round(dt / n_it * iters * nrhs, 1)
+        out["est_basis"] = "%d iterations x %d right-hand sides" % (iters, nrhs)
     return out
 
 
@@ -626,7 +657,8 @@ def main():
         stream = torch.cuda.Stream(device=dev)
         only = [v for v in a.ms_variants.split(",") if v]
         res = msolve_bench(rb, F, np, torch, rank, dev, stream, relative=a.ms_relative, only=only, nrhs=a.ms_nrhs,
-                           nshift=a.ms_nshift, mass=a.ms_mass, warmup=not a.ms_no_warmup)
+                           nshift=a.ms_nshift, mass=a.ms_mass, warmup=not a.ms_no_warmup,
+                           cpu=rank == 0 and world == 1 and not a.no_cpu_baseline)
 
         if rank == 0:
             print(json.dumps({"workload": "msolve", "n_gpus": world, "data": "synthetic", **res}))
@@ -722,12 +754,13 @@ def main():
 
     ms = ms32 = None
     if not a.no_msolve:
+        cpu_ms = rank == 0 and world == 1 and not a.no_cpu_baseline
         try:
-            ms = msolve_bench(rb, F, np, torch, rank, dev, stream)
+            ms = msolve_bench(rb, F, np, torch, rank, dev, stream, cpu=cpu_ms)
         except Exception as e:  # reported in the JSON line, the Dslash numbers stand
             ms = {"error": str(e)[:300]}
         try:
-            ms32 = msolve_bench(rb, F, np, torch, rank, dev, stream, dims=(32, 32, 32, 32), relative=True)
+            ms32 = msolve_bench(rb, F, np, torch, rank, dev, stream, dims=(32, 32, 32, 32), relative=True, cpu=cpu_ms)
         except Exception as e:
             ms32 = {"error": str(e)[:300]}
 
