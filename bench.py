@@ -268,8 +268,10 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False,
     free, total = torch.cuda.mem_get_info(dev)
     out["device_memory_in_use_gb"] = round((total - free) / 1e9, 2)  # workspaces of all variants, at the end
     ctx.close()
-    tag = {(24, 24, 24, 32): "m24", (32, 32, 32, 32): "m32"}.get(tuple(dims))
-    if cpu and tag and nshift == 16 and abs(mass - 0.01) < 1e-12:
+    # the bounded reference builds: lattice -> (tag, poles, mass) they were compiled for
+    tag, ref_nshift, ref_mass = {(24, 24, 24, 32): ("m24", 16, 0.01), (32, 32, 32, 32): ("m32", 16, 0.01),
+                                 (48, 48, 48, 48): ("m48", 20, 0.005)}.get(tuple(dims), (None, 0, 0.0))
+    if cpu and tag and nshift == ref_nshift and abs(mass - ref_mass) < 1e-12:
         out["cpu_reference"] = reference_msolve_timing(tag, u, b_host[0], shifts, np,
                                                        out.get("fp64_single_rhs", {}).get("iters", [None])[0], nrhs)
     return out
@@ -278,7 +280,7 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False,
 def reference_msolve_timing(tag, u, b, shifts, np, iters, nrhs):
     """The reference's own CPU multi-shift solver (multips_shifted_invert,
     lib/Action/Inverter/inverter.cc:142-339, unmodified, behind the harness in
-    oracle/_ref/libref_<tag>.so, built with max_cg = 100 (24^3x32) or 60 (32^4)) on the same links,
+    oracle/_ref/libref_<tag>.so, built with max_cg = 100 (24^3x32), 60 (32^4) or 10 (48^4)) on the same links,
     right-hand side and poles, on one host core: seconds per iteration over its first max_cg
     iterations (all 16 poles still active, so an upper figure for the average iteration), and
     that figure times the B200 solve's iteration count as the estimated CPU time of the solve."""
@@ -295,7 +297,7 @@ def reference_msolve_timing(tag, u, b, shifts, np, iters, nrhs):
     ref.msolve(1e-10, shifts)
     dt = time.perf_counter() - t0
     out = {"kind": "reference", "cores": 1, "iterations_timed": n_it, "s_per_iteration": round(dt / n_it, 5),
-           "sample": "first %d iterations of one right-hand side, 16 poles, FP64" % n_it}
+           "sample": "first %d iterations of one right-hand side, %d poles, FP64" % (n_it, len(shifts))}
     if iters:
         out["est_s_per_solve"] = round(dt / n_it * iters * nrhs, 1)
         out["est_basis"] = "%d iterations x %d right-hand sides" % (iters, nrhs)
