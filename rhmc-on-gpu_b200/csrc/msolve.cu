@@ -26,7 +26,7 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     const size_t vbytes = stride * sizeof(E);
     const int S = A.nshift;
     void *r, *p, *h, *s, *ps, *stv, *part, *tick;
-    CK(c->ws.get("ms_r", NR * vbytes, &r));
+    CK(c->ws.get("ms_r", (size_t)MS_WIN * NR * vbytes, &r));  // ring of the window's residuals [slot][rhs]
     CK(c->ws.get("ms_p", NR * vbytes, &p));
     CK(c->ws.get("ms_h", NR * vbytes, &h));
     CK(c->ws.get("ms_s", NR * vbytes, &s));
@@ -54,6 +54,7 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     for (int i = 0; i < S; i++) h0.tgt[i] = A.tgt[i];
     for (int r = 0; r < NR; r++)
         for (int i = 0; i < S; i++) h0.rhs[r].shift[i] = A.shift[(size_t)r * S + i] - A.base[r];
+    h0.wpos = 0;
     CK(cudaMemcpyAsync(st, &h0, sizeof(MSState), cudaMemcpyHostToDevice, s_));
     CK(cudaMemsetAsync(tk, 0, 4 * sizeof(unsigned), s_));
 
@@ -92,7 +93,7 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
     a2.fin.st = st;
     a2.stop = &st->stop;
 
-    const int chunk = A.chunk > 0 ? A.chunk : 8;
+    const int chunk = MS_WIN;  // one graph replay = one delayed-update window
     struct Key {
         int kind, link_reals, link_bytes, nr, chunk, nshift, vh;
         const void *links, *r, *p, *h, *s, *ps, *xs, *pt, *tk, *st;
@@ -100,7 +101,7 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
         cudaStream_t stream;
     } key;
     memset(&key, 0, sizeof(key));
-    key.kind = 1; key.link_reals = LF::reals; key.link_bytes = (int)sizeof(typename LF::real); key.nr = NR;
+    key.kind = 4; key.link_reals = LF::reals; key.link_bytes = (int)sizeof(typename LF::real); key.nr = NR;
     key.chunk = chunk; key.nshift = S; key.vh = Vh; key.links = lf.p; key.r = r; key.p = p; key.h = h; key.s = s;
     key.ps = ps; key.xs = xs; key.pt = pt; key.tk = tk; key.st = st; key.stream = s_;
     for (int r = 0; r < NR; r++) key.alpha[r] = (double)a2.alphas[r];
@@ -114,8 +115,9 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
             dslash_kernel<LF, NR, false, false, NoFin><<<gd1, DslashCfg<LF, NR, false>::block, 0, s_>>>(a1);
             dslash_kernel<LF, NR, true, true, FinAlpha<NR>><<<gd2, DslashCfg<LF, NR, true>::block, 0, s_>>>(a2);
             ms_resid_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)r, (const E *)s, pt, tk + 2, st);
-            ms_update_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, S, stride, (const E *)r, (E *)p, (E *)ps, xs, st);
+            ms_update_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)r, (E *)p, st);
         }
+        ms_flush_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, S, stride, (const E *)r, (E *)ps, xs, pt, tk + 3, st);
         ce = cudaStreamEndCapture(s_, &graph);
         if (ce != cudaSuccess) return cuda_fail(ce, "msolve capture");
         ce = cudaGraphInstantiate(&exec, graph, 0);
@@ -143,7 +145,7 @@ static int ms_run_nr(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo 
         }
     }
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s_);
-    c->launches += launched * chunk * 4;
+    c->launches += launched * (chunk * 4 + 1);
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
     if (ce != cudaSuccess) return cuda_fail(ce, "msolve loop");

@@ -30,6 +30,7 @@ namespace rhmc {
 
 constexpr int MS_MAX_SHIFT = 32;
 constexpr int MS_MAX_RHS = 8;
+constexpr int MS_WIN = 8;  // iterations per delayed-update window (= iterations per graph replay)
 constexpr int VEC_BLOCK = 256;
 
 struct MSRhs {
@@ -42,11 +43,16 @@ struct MSRhs {
     int active[MS_MAX_SHIFT];       // shift updated in this iteration
     int active_next[MS_MAX_SHIFT];  // after the freezing test
     double shift[MS_MAX_SHIFT];     // sigma_{r,i} - sigma_{r,0}: this RHS's poles relative to its base
+    // the scalars of each iteration m of the current window, for the delayed shifted updates:
+    // x_i -= h_om p_i, then p_i = h_ze r_m + h_ga p_i, applied by ms_flush_kernel when h_act
+    double h_om[MS_MAX_SHIFT][MS_WIN], h_ga[MS_MAX_SHIFT][MS_WIN], h_ze[MS_MAX_SHIFT][MS_WIN];
+    int h_act[MS_MAX_SHIFT][MS_WIN];
 };
 
 struct MSState {
     int stop;     // every RHS finished: K1-K3 skip
     int stop_k4;  // set by the first skipped K1 so that K4 skips from the next iteration on
+    int wpos;     // iterations done in the current window (the residual of iteration m is in ring slot m-1)
     int status;   // 0 ok, 1 iteration cap, 2 non-finite reduction
     int nshift, nrhs, max_iter;
     int stop_on_frozen;             // also stop when every shift is frozen
@@ -102,12 +108,14 @@ struct FinAlpha {
         for (int r = 0; r < NR; r++) {
             MSRhs &q = st->rhs[r];
             q.running = q.running_next;
+            for (int i = 0; i < st->nshift; i++) q.h_act[i][st->wpos] = q.running ? q.active_next[i] : 0;
             if (!q.running) continue;
             for (int i = 0; i < st->nshift; i++) q.active[i] = q.active_next[i];
             q.alpha = tot[r];
             if (!isfinite(q.alpha) || q.alpha == 0.0) {
                 st->status = 2;
                 st->stop = 1;
+                for (int i = 0; i < st->nshift; i++) q.h_act[i][st->wpos] = 0;
                 q.running = 0;
                 q.running_next = 0;
                 continue;
@@ -121,6 +129,7 @@ struct FinAlpha {
                                     (q.omega * q.gamma * (zi - zii) + zi * q.omega_prev * (1.0 - q.shift[i] * q.omega));
                 q.zeta_iii[i] = ziii;
                 q.omegas[i] = q.omega * ziii / zii;
+                q.h_om[i][st->wpos] = q.omegas[i];
             }
         }
     }
@@ -146,6 +155,8 @@ struct FinLambda {
             for (int i = 0; i < st->nshift; i++) {
                 if (!q.active[i]) continue;
                 q.gammas[i] = q.gamma * q.zeta_iii[i] * q.omegas[i] / (q.zeta_ii[i] * q.omega);
+                q.h_ga[i][st->wpos] = q.gammas[i];
+                q.h_ze[i][st->wpos] = q.zeta_iii[i];
                 const double fact = sqrt(q.delta * q.zeta_ii[i] * q.zeta_ii[i]);
                 q.active_next[i] = (fact < st->tgt[i]) ? 0 : 1;
                 nact += q.active_next[i];
@@ -164,7 +175,14 @@ struct FinLambda {
         }
         for (int r = NR; r < st->nrhs; r++) any |= st->rhs[r].running_next;
         if (!any) st->stop = 1;
+        st->wpos++;
     }
+};
+
+// end of a window (after ms_flush_kernel has read its scalars)
+struct FinWindow {
+    MSState *st;
+    __device__ void operator()(const double *) const { st->wpos = 0; }
 };
 
 // ------------------------------------------------------------------ vector kernels
@@ -173,13 +191,15 @@ struct MSVec {
     typedef typename SpinorT<Rv>::elem E;
 };
 
-// x_i = 0, r = p = p_i = b (b FP64 internal), |b|^2
+// x_i = 0, r_0 = p = p_i = b (b FP64 internal), |b|^2.  r_0 goes to the last slot of the
+// residual ring (the slot the first iteration reads).
 template <typename Rv, int NR>
 __global__ void __launch_bounds__(VEC_BLOCK) ms_init_kernel(int Vh, int nshift, size_t stride, const double2 *__restrict__ b,
-                                                             typename MSVec<Rv>::E *r, typename MSVec<Rv>::E *p,
+                                                             typename MSVec<Rv>::E *ring, typename MSVec<Rv>::E *p,
                                                              typename MSVec<Rv>::E *ps, typename MSVec<Rv>::E *x,
                                                              double *partials, unsigned *ticket, MSState *st)
 {
+    typename MSVec<Rv>::E *r = ring + (size_t)(MS_WIN - 1) * NR * stride;
     typedef typename MSVec<Rv>::E E;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double red[NR];
@@ -213,14 +233,17 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_init_kernel(int Vh, int nshift, 
     reduce_finalize<NR>(red, partials, ticket, fin);
 }
 
-// r += omega s, |r|^2 per RHS
+// r_m = r_{m-1} + omega s (ring slots wpos-1 -> wpos), |r_m|^2 per RHS
 template <typename Rv, int NR>
-__global__ void __launch_bounds__(VEC_BLOCK) ms_resid_kernel(int Vh, size_t stride, typename MSVec<Rv>::E *r,
+__global__ void __launch_bounds__(VEC_BLOCK) ms_resid_kernel(int Vh, size_t stride, typename MSVec<Rv>::E *ring,
                                                               const typename MSVec<Rv>::E *__restrict__ s, double *partials,
                                                               unsigned *ticket, MSState *st)
 {
     typedef typename MSVec<Rv>::E E;
     if (*(volatile int *)&st->stop) return;
+    const int wp = *(volatile const int *)&st->wpos;
+    const E *rprev = ring + (size_t)((wp + MS_WIN - 1) % MS_WIN) * NR * stride;
+    E *r = ring + (size_t)wp * NR * stride;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double red[NR];
 #pragma unroll
@@ -233,7 +256,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_resid_kernel(int Vh, size_t stri
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const size_t o = j * stride + (size_t)c * Vh + k;
-                E rv = r[o];
+                E rv = rprev[o];
                 const E sv = s[o];
                 rv.x = rv.x + om * sv.x;
                 rv.y = rv.y + om * sv.y;
@@ -246,66 +269,117 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_resid_kernel(int Vh, size_t stri
     reduce_finalize<NR>(red, partials, ticket, fin);
 }
 
-// p = r + gamma p ; x_i -= omega_i p_i ; p_i = zeta'''_i r + gamma_i p_i
+// p = r_m + gamma p (the base search direction; the shifted p_i and x_i are updated once per
+// window by ms_flush_kernel)
 template <typename Rv, int NR>
-__global__ void __launch_bounds__(VEC_BLOCK) ms_update_kernel(int Vh, int nshift, size_t stride,
-                                                               const typename MSVec<Rv>::E *__restrict__ r,
-                                                               typename MSVec<Rv>::E *p, typename MSVec<Rv>::E *ps,
-                                                               typename MSVec<Rv>::E *x, MSState *st)
+__global__ void __launch_bounds__(VEC_BLOCK) ms_update_kernel(int Vh, size_t stride, const typename MSVec<Rv>::E *__restrict__ ring,
+                                                               typename MSVec<Rv>::E *p, MSState *st)
 {
     typedef typename MSVec<Rv>::E E;
-    __shared__ Rv s_om[NR][MS_MAX_SHIFT], s_ze[NR][MS_MAX_SHIFT], s_ga[NR][MS_MAX_SHIFT];
-    __shared__ int s_act[NR][MS_MAX_SHIFT];
-    __shared__ Rv s_gamma[NR];
-    __shared__ int s_run[NR];
     if (*(volatile int *)&st->stop_k4) return;
-    for (int t = threadIdx.x; t < NR * MS_MAX_SHIFT; t += blockDim.x) {
-        const int j = t / MS_MAX_SHIFT, i = t % MS_MAX_SHIFT;
-        const MSRhs &q = st->rhs[j];
-        s_act[j][i] = (i < nshift) ? q.active[i] : 0;
-        s_om[j][i] = (Rv)q.omegas[i];
-        s_ze[j][i] = (Rv)q.zeta_iii[i];
-        s_ga[j][i] = (Rv)q.gammas[i];
-        if (i == 0) {
-            s_gamma[j] = (Rv)q.gamma;
-            s_run[j] = q.running;
-        }
-    }
-    __syncthreads();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= Vh) return;
+    const E *r = ring + (size_t)((*(volatile const int *)&st->wpos + MS_WIN - 1) % MS_WIN) * NR * stride;
 #pragma unroll
     for (int j = 0; j < NR; j++) {
-        if (!s_run[j]) continue;
-        E rv[3];
-        const Rv g = s_gamma[j];
+        const MSRhs &q = st->rhs[j];
+        if (!q.running) continue;
+        const Rv g = (Rv)q.gamma;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const size_t o = j * stride + (size_t)c * Vh + k;
-            rv[c] = r[o];
+            const E rv = r[o];
             E pv = p[o];
-            pv.x = rv[c].x + g * pv.x;
-            pv.y = rv[c].y + g * pv.y;
+            pv.x = rv.x + g * pv.x;
+            pv.y = rv.y + g * pv.y;
             p[o] = pv;
         }
-        for (int i = 0; i < nshift; i++) {
-            if (!s_act[j][i]) continue;
-            const Rv om = s_om[j][i], ze = s_ze[j][i], ga = s_ga[j][i];
-            const size_t base = (size_t)(j * nshift + i) * stride + k;
+    }
+}
+
+// End of a window of m = wpos iterations with residuals r_1..r_m (ring slots 0..m-1).  Over the
+// window the per-iteration updates x_i -= om_k p_i, p_i = ze_k r_k + ga_k p_i compose to
+//   x_i = X0_i - cx0 P0_i - sum_k cx_k r_k,   p_i = ca P0_i + sum_k cb_k r_k
+// with P0_i, X0_i the stored vectors of the window start.  The first NR*nshift threads of every
+// block derive (cx0, cx, ca, cb) of one (rhs, shift) from the recorded scalars into shared memory
+// (skipping iterations where the shift was frozen), then every site applies them: each shifted
+// vector is read and written once per window instead of once per iteration.
+template <typename Rv, int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) ms_flush_kernel(int Vh, int nshift, size_t stride,
+                                                              const typename MSVec<Rv>::E *__restrict__ ring,
+                                                              typename MSVec<Rv>::E *ps, typename MSVec<Rv>::E *x,
+                                                              double *partials, unsigned *ticket, MSState *st)
+{
+    typedef typename MSVec<Rv>::E E;
+    __shared__ double s_cx0[NR * MS_MAX_SHIFT], s_ca[NR * MS_MAX_SHIFT];
+    __shared__ double s_cx[NR * MS_MAX_SHIFT][MS_WIN], s_cb[NR * MS_MAX_SHIFT][MS_WIN];
+    __shared__ int s_use[NR * MS_MAX_SHIFT];  // 0: nothing to do, 1: x only, 2: x and p
+    const int wp = *(volatile const int *)&st->wpos;
+    for (int t = threadIdx.x; t < NR * nshift; t += blockDim.x) {
+        const int j = t / nshift, i = t % nshift;
+        const MSRhs &q = st->rhs[j];
+        double cx0 = 0.0, ca = 1.0, cx[MS_WIN], cb[MS_WIN];
+        int any = 0;
+        for (int m = 0; m < MS_WIN; m++) cx[m] = cb[m] = 0.0;
+        for (int m = 0; m < wp; m++) {
+            if (!q.h_act[i][m]) continue;
+            any = 1;
+            const double om = q.h_om[i][m], ga = q.h_ga[i][m];
+            cx0 += om * ca;
+            for (int l = 0; l < m; l++) cx[l] += om * cb[l];
+            ca *= ga;
+            for (int l = 0; l < m; l++) cb[l] *= ga;
+            cb[m] = q.h_ze[i][m];
+        }
+        s_cx0[t] = cx0;
+        s_ca[t] = ca;
+        for (int m = 0; m < MS_WIN; m++) {
+            s_cx[t][m] = cx[m];
+            s_cb[t][m] = cb[m];
+        }
+        s_use[t] = any ? ((q.running_next && q.active_next[i]) ? 2 : 1) : 0;
+    }
+    __syncthreads();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < Vh && wp > 0) {
+        for (int j = 0; j < NR; j++) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const size_t o = base + (size_t)c * Vh;
-                E pv = ps[o];
-                E xv = x[o];
-                xv.x = xv.x - om * pv.x;
-                xv.y = xv.y - om * pv.y;
-                pv.x = ze * rv[c].x + ga * pv.x;
-                pv.y = ze * rv[c].y + ga * pv.y;
-                x[o] = xv;
-                ps[o] = pv;
+                // the window's residuals of this site, read once and shared by every shift
+                E rv[MS_WIN];
+#pragma unroll
+                for (int m = 0; m < MS_WIN; m++)
+                    if (m < wp) rv[m] = ring[((size_t)m * NR + j) * stride + (size_t)c * Vh + k];
+                for (int i = 0; i < nshift; i++) {
+                    const int t = j * nshift + i, use = s_use[t];
+                    if (!use) continue;
+                    const size_t o = (size_t)t * stride + (size_t)c * Vh + k;
+                    const Rv x0 = (Rv)s_cx0[t], a0 = (Rv)s_ca[t];
+                    const E p0 = ps[o];
+                    E xv = x[o];
+                    E pv;
+                    xv.x = xv.x - x0 * p0.x;
+                    xv.y = xv.y - x0 * p0.y;
+                    pv.x = a0 * p0.x;
+                    pv.y = a0 * p0.y;
+#pragma unroll
+                    for (int m = 0; m < MS_WIN; m++) {
+                        if (m >= wp) break;
+                        const Rv cx = (Rv)s_cx[t][m], cb = (Rv)s_cb[t][m];
+                        xv.x = xv.x - cx * rv[m].x;
+                        xv.y = xv.y - cx * rv[m].y;
+                        pv.x = pv.x + cb * rv[m].x;
+                        pv.y = pv.y + cb * rv[m].y;
+                    }
+                    x[o] = xv;
+                    if (use == 2) ps[o] = pv;
+                }
             }
         }
     }
+    double none[1] = {0.0};
+    FinWindow fin{st};
+    reduce_finalize<1>(none, partials, ticket, fin);
 }
 
 }  // namespace rhmc
