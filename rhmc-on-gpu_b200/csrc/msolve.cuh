@@ -66,6 +66,7 @@ struct FinInit {
     MSState *st;
     __device__ void operator()(const double *tot) const
     {
+        if (threadIdx.x != 0) return;
         for (int r = 0; r < st->nrhs; r++) {
             MSRhs &q = st->rhs[r];
             q.b2 = tot[r];
@@ -100,37 +101,47 @@ struct FinInit {
     }
 };
 
+// FinAlpha and FinLambda run in every thread of the reduction's last block: thread 0 steps the
+// scalars of each right-hand side, then one thread per (rhs, shift) the shifted recurrences
+// (independent divisions in parallel instead of one thread's serial chain).
 template <int NR>
 struct FinAlpha {
     MSState *st;
     __device__ void operator()(const double *tot) const
     {
-        for (int r = 0; r < NR; r++) {
+        if (threadIdx.x == 0) {
+            for (int r = 0; r < NR; r++) {
+                MSRhs &q = st->rhs[r];
+                q.running = q.running_next;
+                if (!q.running) continue;
+                q.alpha = tot[r];
+                if (!isfinite(q.alpha) || q.alpha == 0.0) {
+                    st->status = 2;
+                    st->stop = 1;
+                    q.running = 0;
+                    q.running_next = 0;
+                    continue;
+                }
+                q.omega_prev = q.omega;
+                q.omega = -q.delta / q.alpha;
+            }
+        }
+        __syncthreads();
+        const int ns = st->nshift, wp = st->wpos;
+        for (int t = threadIdx.x; t < NR * ns; t += blockDim.x) {
+            const int r = t / ns, i = t % ns;
             MSRhs &q = st->rhs[r];
-            q.running = q.running_next;
-            for (int i = 0; i < st->nshift; i++) q.h_act[i][st->wpos] = q.running ? q.active_next[i] : 0;
+            const int act = q.running ? q.active_next[i] : 0;
+            q.h_act[i][wp] = act;
             if (!q.running) continue;
-            for (int i = 0; i < st->nshift; i++) q.active[i] = q.active_next[i];
-            q.alpha = tot[r];
-            if (!isfinite(q.alpha) || q.alpha == 0.0) {
-                st->status = 2;
-                st->stop = 1;
-                for (int i = 0; i < st->nshift; i++) q.h_act[i][st->wpos] = 0;
-                q.running = 0;
-                q.running_next = 0;
-                continue;
-            }
-            q.omega_prev = q.omega;
-            q.omega = -q.delta / q.alpha;
-            for (int i = 0; i < st->nshift; i++) {
-                if (!q.active[i]) continue;
-                const double zi = q.zeta_i[i], zii = q.zeta_ii[i];
-                const double ziii = (zi * zii * q.omega_prev) /
-                                    (q.omega * q.gamma * (zi - zii) + zi * q.omega_prev * (1.0 - q.shift[i] * q.omega));
-                q.zeta_iii[i] = ziii;
-                q.omegas[i] = q.omega * ziii / zii;
-                q.h_om[i][st->wpos] = q.omegas[i];
-            }
+            q.active[i] = act;
+            if (!act) continue;
+            const double zi = q.zeta_i[i], zii = q.zeta_ii[i];
+            const double ziii = (zi * zii * q.omega_prev) /
+                                (q.omega * q.gamma * (zi - zii) + zi * q.omega_prev * (1.0 - q.shift[i] * q.omega));
+            q.zeta_iii[i] = ziii;
+            q.omegas[i] = q.omega * ziii / zii;
+            q.h_om[i][wp] = q.omegas[i];
         }
     }
 };
@@ -140,29 +151,41 @@ struct FinLambda {
     MSState *st;
     __device__ void operator()(const double *tot) const
     {
+        if (threadIdx.x == 0) {
+            for (int r = 0; r < NR; r++) {
+                MSRhs &q = st->rhs[r];
+                if (!q.running) continue;
+                q.lambda = tot[r];
+                if (!isfinite(q.lambda)) {
+                    st->status = 2;
+                    q.running_next = 0;
+                    continue;
+                }
+                q.gamma = q.lambda / q.delta;
+            }
+        }
+        __syncthreads();
+        const int ns = st->nshift, wp = st->wpos;
+        for (int t = threadIdx.x; t < NR * ns; t += blockDim.x) {
+            const int r = t / ns, i = t % ns;
+            MSRhs &q = st->rhs[r];
+            if (!q.running || !isfinite(q.lambda) || !q.active[i]) continue;
+            q.gammas[i] = q.gamma * q.zeta_iii[i] * q.omegas[i] / (q.zeta_ii[i] * q.omega);
+            q.h_ga[i][wp] = q.gammas[i];
+            q.h_ze[i][wp] = q.zeta_iii[i];
+            const double fact = sqrt(q.delta * q.zeta_ii[i] * q.zeta_ii[i]);
+            q.active_next[i] = (fact < st->tgt[i]) ? 0 : 1;
+            q.zeta_i[i] = q.zeta_ii[i];
+            q.zeta_ii[i] = q.zeta_iii[i];
+        }
+        __syncthreads();
+        if (threadIdx.x != 0) return;
         int any = 0;
         for (int r = 0; r < NR; r++) {
             MSRhs &q = st->rhs[r];
-            if (!q.running) continue;
-            q.lambda = tot[r];
-            if (!isfinite(q.lambda)) {
-                st->status = 2;
-                q.running_next = 0;
-                continue;
-            }
-            q.gamma = q.lambda / q.delta;
+            if (!q.running || !isfinite(q.lambda)) continue;
             int nact = 0;
-            for (int i = 0; i < st->nshift; i++) {
-                if (!q.active[i]) continue;
-                q.gammas[i] = q.gamma * q.zeta_iii[i] * q.omegas[i] / (q.zeta_ii[i] * q.omega);
-                q.h_ga[i][st->wpos] = q.gammas[i];
-                q.h_ze[i][st->wpos] = q.zeta_iii[i];
-                const double fact = sqrt(q.delta * q.zeta_ii[i] * q.zeta_ii[i]);
-                q.active_next[i] = (fact < st->tgt[i]) ? 0 : 1;
-                nact += q.active_next[i];
-                q.zeta_i[i] = q.zeta_ii[i];
-                q.zeta_ii[i] = q.zeta_iii[i];
-            }
+            for (int i = 0; i < ns; i++) nact += q.active[i] ? q.active_next[i] : 0;
             q.delta = q.lambda;
             q.iter++;
             int done = (sqrt(q.lambda) <= st->res) || (st->stop_on_frozen && nact == 0);
@@ -182,7 +205,10 @@ struct FinLambda {
 // end of a window (after ms_flush_kernel has read its scalars)
 struct FinWindow {
     MSState *st;
-    __device__ void operator()(const double *) const { st->wpos = 0; }
+    __device__ void operator()(const double *) const
+    {
+        if (threadIdx.x == 0) st->wpos = 0;
+    }
 };
 
 // ------------------------------------------------------------------ vector kernels

@@ -91,6 +91,7 @@ struct FinRU {
     RBState *st;
     __device__ void operator()(const double *tot) const
     {
+        if (threadIdx.x != 0) return;
         int all = 1;
         for (int j = 0; j < NR; j++) {
             if (st->conv[j]) continue;
@@ -156,6 +157,7 @@ struct FinRBAlpha {
     RBState *st;
     __device__ void operator()(const double *tot) const
     {
+        if (threadIdx.x != 0) return;
         for (int j = 0; j < NR; j++) {
             const double pap = tot[j];
             st->hold[j] = st->pending[j];
@@ -172,6 +174,7 @@ struct FinRBBeta {
     RBState *st;
     __device__ void operator()(const double *tot) const
     {
+        if (threadIdx.x != 0) return;
         for (int j = 0; j < NR; j++) {
             if (st->conv[j] || st->hold[j]) { st->beta[j] = 0.0; continue; }
             const double rn = tot[j];

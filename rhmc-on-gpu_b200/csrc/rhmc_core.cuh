@@ -427,8 +427,8 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double *smem)
 // and chunk instead of one per value and warp).  Every block writes one partial per chunk it
 // covers (blockDim must be 128 or 256); the last block to finish (atomic ticket) sums the chunk
 // partials with its first 128 threads (thread t takes chunks t, t+128, ... in order), then a
-// shuffle tree per warp and the 4 warp sums in order, hands the totals to fin() in thread 0 and
-// re-arms the ticket.  A batched launch (NR right-hand sides, 128-thread blocks) therefore
+// shuffle tree per warp and the 4 warp sums in order, re-arms the ticket and hands the totals to
+// fin(), which every thread of that block calls (a finaliser may split its work across them).  A batched launch (NR right-hand sides, 128-thread blocks) therefore
 // reduces each RHS bit for bit as a single-RHS launch (256-thread blocks) does.
 // All threads of every block must call it.  partials: red_chunks(n) * N doubles.
 struct NoFin {
@@ -476,16 +476,17 @@ __device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials
 #pragma unroll
     for (int j = 0; j < N; j++) acc[j] = 0.0;
     if (threadIdx.x < RED_CHUNK) {
-        // chunks t, t+128, ... added in that order; 4 chunks' loads are issued together
+        // chunks t, t+128, ... added in that order; the loads of B chunks are issued together
+        constexpr int B = (N <= 4) ? 8 : 4;
         int i = threadIdx.x;
-        for (; i + 3 * RED_CHUNK < nch; i += 4 * RED_CHUNK) {
-            double q[4][N];
+        for (; i + (B - 1) * RED_CHUNK < nch; i += B * RED_CHUNK) {
+            double q[B][N];
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+            for (int u = 0; u < B; u++)
 #pragma unroll
                 for (int j = 0; j < N; j++) q[u][j] = __ldcg(partials + (size_t)(i + u * RED_CHUNK) * N + j);
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+            for (int u = 0; u < B; u++)
 #pragma unroll
                 for (int j = 0; j < N; j++) acc[j] += q[u][j];
         }
@@ -499,8 +500,8 @@ __device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials
 #pragma unroll
         for (int j = 0; j < N; j++) sm[j][wid] = acc[j];
     __syncthreads();
+    __shared__ double tot[N];
     if (threadIdx.x == 0) {
-        double tot[N];
 #pragma unroll
         for (int j = 0; j < N; j++) {
             double t = sm[j][0];
@@ -510,8 +511,9 @@ __device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials
             tot[j] = t;
         }
         *ticket = 0;
-        fin(tot);
     }
+    __syncthreads();
+    fin(tot);
 }
 
 }  // namespace rhmc
