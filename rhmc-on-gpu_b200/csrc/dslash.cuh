@@ -69,6 +69,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
     if (a.run_if && *(volatile const int *)a.run_if == 0) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int Vh = a.g.Vh;
+    // y (read only by the epilogue) is fetched into shared memory by cp.async at the start, so its
+    // DRAM latency overlaps the stencil instead of following it (when the block's copy fits)
+    typedef typename LF::store S;
+    typedef typename S::elem E;
+    constexpr bool PF = HAS_Y && (NR * S::planes * BLOCK * sizeof(E) <= 24576);
+    __shared__ __align__(16) E ysm[PF ? NR * S::planes * BLOCK : 1];
+    if (PF && k < Vh) {
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+#pragma unroll
+            for (int pl = 0; pl < S::planes; pl++)
+                cp_async_elem<sizeof(E)>(&ysm[(r * S::planes + pl) * BLOCK + threadIdx.x],
+                                         a.y + r * a.stride + (size_t)pl * Vh + k);
+        cp_async_commit();
+    }
     double red[NR];
 #pragma unroll
     for (int j = 0; j < NR; j++) red[j] = 0.0;
@@ -102,7 +117,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
         for (int r = 0; r < NR; r++) {
             vec3<R> o;
             if (HAS_Y) {
-                vec3<R> yv = LF::store::template load<R>(a.y + r * a.stride, Vh, k);
+                if (PF && r == 0) cp_async_wait_all();
+                const vec3<R> yv = PF ? S::template load_plain<R>(ysm + r * S::planes * BLOCK, BLOCK, threadIdx.x)
+                                      : S::template load<R>(a.y + r * a.stride, Vh, k);
                 const R al = a.use_alphas ? a.alphas[r] : a.alpha;
 #pragma unroll
                 for (int c = 0; c < 3; c++)

@@ -295,6 +295,18 @@ struct F64S {
         for (int c = 0; c < 3; c++) d.c[c] = mk<double>((double)r.c[c].re, (double)r.c[c].im);
         store_spinor<double>(v, Vh, k, d);
     }
+    // the same from memory that __ldg cannot address (shared), planes pstride elements apart
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> load_plain(const elem *v, int pstride, int k)
+    {
+        vec3<R> r;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const elem a = v[c * pstride + k];
+            r.c[c] = mk<R>((R)a.x, (R)a.y);
+        }
+        return r;
+    }
 };
 
 struct F32S {
@@ -318,6 +330,17 @@ struct F32S {
         for (int c = 0; c < 3; c++) f.c[c] = mk<float>((float)r.c[c].re, (float)r.c[c].im);
         store_spinor<float>(v, Vh, k, f);
     }
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> load_plain(const elem *v, int pstride, int k)
+    {
+        vec3<R> r;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const elem a = v[c * pstride + k];
+            r.c[c] = mk<R>((R)a.x, (R)a.y);
+        }
+        return r;
+    }
 };
 
 // Half precision with a per-site scale, one 16-byte vector per site: words x, y, z hold the
@@ -337,7 +360,16 @@ struct H16S {
     template <typename R>
     __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int, int k)
     {
-        const uint4 q = __ldg(v + k);
+        return decode<R>(__ldg(v + k));
+    }
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> load_plain(const elem *v, int, int k)
+    {
+        return decode<R>(v[k]);
+    }
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> decode(const uint4 q)
+    {
         const float nrm = __uint_as_float(q.w);
         const float2 f0 = h2f(q.x), f1 = h2f(q.y), f2 = h2f(q.z);
         vec3<R> r;
@@ -361,6 +393,21 @@ struct H16S {
         v[k] = q;
     }
 };
+
+// asynchronous global -> shared copy of one element (cp.async: no registers held while in flight)
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem)
+{
+    static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async copies 4, 8 or 16 bytes");
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    const size_t ga = __cvta_generic_to_global(gmem);
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(ga) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(ga), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // ------------------------------------------------------------------ SU(3) x vector
 // acc += U v
