@@ -526,6 +526,90 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
     return out
 
 
+B5_ML, B5_MS, B5_BETA, B5_DEG = 0.005, 0.04, 5.8, 20
+
+
+def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
+    """Large batched RHMC: N_f = 2+1 staggered (light am=0.005 with N_f=2, strange am=0.04 with
+    N_f=1) on b5_dims (48^4 by default), beta=5.8, degree-20 rational approximations per pole set,
+    b5_ps pseudofermions per species (4 + 4 = 8 right-hand sides: the two species have the same
+    pole count, so every multi-shift solve runs all 8 together), start exp(i 0.3 H) per link
+    (seed 1001), momenta seed 3003, phi seeds 2002/2003, Metropolis uniform seed 4004; synthetic
+    data.  One leapfrog trajectory (tau = 1, b5_steps steps; force solves to 1e-8, heatbath and
+    action solves to 1e-10) three times: every solve in plain FP64 (18-real links) one
+    pseudofermion at a time (the reference's loop), the same with all right-hand sides batched,
+    and every solve in the mixed batched solver (FP64 12-real multi-shift + FP32 refinement, same
+    targets): seconds per trajectory, Delta H, acceptance, plaquette and device memory in use."""
+    from rhmc_b200 import rational as R
+    from rhmc_b200 import replicas as RP
+    torch.cuda.set_stream(stream)
+    dims = tuple(int(d) for d in a.b5_dims.split(","))
+    nps = a.b5_ps
+    ctx = rb.Context(dims, mass=B5_ML, beta=B5_BETA, device=dev.index or 0)
+    ctx.set_stream(stream.cuda_stream)
+    u0 = F.random_links(dims, seed=RP.replica_seed(1001, rank), kind="near1", eps=0.3)
+    ctx.set_gauge(u0)
+    P0 = F.random_momenta(dims, seed=RP.replica_seed(3003, rank))
+    phis = [F.random_spinor(dims, seed=RP.replica_seed(2002 + s, rank), n=nps) for s in range(2)]
+    uniform = float(np.random.Generator(np.random.Philox(RP.replica_seed(4004, rank))).random())
+    lmax = ctx.find_max(F.random_spinor(dims, seed=7007))
+    species = [(B5_ML, 2), (B5_MS, 1)]
+    bounds, approx = [], []
+    for m, nf in species:
+        lo, hi = m * m, lmax + m * m - B5_ML * B5_ML
+        eps = 0.95 * lo / (1.05 * hi)
+        bounds.append((lo, hi))
+        approx.append([R.rational_power(nf / (8.0 * nps), B5_DEG, eps), R.rational_power(-nf / (4.0 * nps), B5_DEG, eps),
+                       R.rational_power(-nf / (4.0 * nps), B5_DEG, eps)])
+    out = {"config": {"lattice": list(dims), "beta": B5_BETA,
+                      "species": [{"mass": m, "no_flavours": nf, "no_ps": nps} for m, nf in species],
+                      "rhs_batched": 2 * nps, "degree": B5_DEG, "eig_bounds": bounds,
+                      "start": "exp(i 0.3 H) of a Gaussian algebra element H per link",
+                      "integrator": "leapfrog tau=1, %d steps; force solves 1e-8, heatbath/action solves 1e-10"
+                                    % a.b5_steps,
+                      "approx_max_rel_err": max(c["max_rel_err"] for ap_ in approx for c in ap_)}}
+    have_ms = False
+    traj = {}
+    arms = (("fp64_single_rhs", rb.MSOLVE_FP64, rb.LINKS_F64_18, 1), ("fp64_batched", rb.MSOLVE_FP64, rb.LINKS_F64_18, 0),
+            ("mixed_batched", rb.MSOLVE_MIXED, rb.LINKS_F64_12, 0))
+    for name, mode, fmt, single in arms:
+        ctx.driver_setup(no_flavours=2, no_ps=nps, no_md=a.b5_steps, integrator=rb.INT_LEAPFROG, residue_metro=1e-10,
+                         residue_md=1e-8, metro_mode=mode, metro_fmt=fmt, md_mode=mode, md_fmt=fmt, single_rhs=single)
+        if not have_ms:
+            ctx.add_species(B5_MS, 1, nps)
+            have_ms = True
+        for s in range(2):
+            ctx.select_species(s)
+            for w in range(3):
+                ctx.set_approx(w, approx[s][w])
+            ctx.set_eig_bounds(*bounds[s])
+            ctx.set_phi(phis[s])
+        ctx.select_species(0)
+        ctx.set_gauge(u0)
+        ctx.set_momenta(P0)
+        stream.synchronize()
+        n0 = ctx.launch_count()
+        t0 = time.perf_counter()
+        dS, acc = ctx.update(uniform)
+        stream.synchronize()
+        dt = time.perf_counter() - t0
+        free, total = torch.cuda.mem_get_info(dev)
+        traj[name] = {"s_per_trajectory": round(dt, 2), "delta_H": dS, "accepted": acc,
+                      "plaquette_after": ctx.plaquette(), "gpu_launches": ctx.launch_count() - n0,
+                      "device_memory_in_use_gb": round((total - free) / 1e9, 2)}
+        print("rhmc48: %s trajectory %.1f s, dH %.6g" % (name, dt, dS), file=sys.stderr, flush=True)
+    for k in ("fp64_batched", "mixed_batched"):
+        traj["speedup_%s_vs_fp64_single_rhs" % k] = round(traj["fp64_single_rhs"]["s_per_trajectory"]
+                                                          / traj[k]["s_per_trajectory"], 3)
+    traj["delta_H_abs_diff_max"] = max(abs(traj[k]["delta_H"] - traj["fp64_single_rhs"]["delta_H"]) for k, *_ in arms)
+    traj["memory_note"] = ("in use after each arm (library workspaces are kept, so this is the high-water mark "
+                           "of the arms run so far)")
+    out["trajectory"] = traj
+    ctx.close()
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    return out
+
+
 def rhmc4_bench(a, rb, F, np, torch, rank, dev, stream):
     """Plain RHMC as the reference CPU build runs it: N_f=2 staggered on 4^4, beta=5.5, am=0.1,
     degree-8 approximations of x^(1/4) (heatbath) and x^(-1/2) (force, action) on [1e-3, 64],
@@ -605,7 +689,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dims", default="32,32,32,32")
     ap.add_argument("--no-msolve", action="store_true")
-    ap.add_argument("--workload", default="dslash", choices=["dslash", "nf2p1", "msolve", "rhmc4"],
+    ap.add_argument("--workload", default="dslash", choices=["dslash", "nf2p1", "msolve", "rhmc4", "rhmc48"],
                     help="dslash: the headline line (Dslash + multi-shift CG); nf2p1: N_f=2+1 forces, "
                          "finite-difference check and trajectories; msolve: the multi-shift CG comparison alone")
     ap.add_argument("--ms-relative", action="store_true", help="msolve workload: residual relative to |b|")
@@ -619,6 +703,9 @@ def main():
     ap.add_argument("--nf-steps", type=int, default=20)
     ap.add_argument("--nf-start", default="near1", choices=["haar", "near1"])
     ap.add_argument("--ms-dims", default="24,24,24,32", help="lattice of the multi-shift CG comparison")
+    ap.add_argument("--b5-dims", default="48,48,48,48", help="rhmc48 workload: lattice")
+    ap.add_argument("--b5-steps", type=int, default=10, help="rhmc48 workload: leapfrog steps per trajectory")
+    ap.add_argument("--b5-ps", type=int, default=4, help="rhmc48 workload: pseudofermions per species")
     a = ap.parse_args()
     a.warmup = max(3, a.warmup)
     if a.impl == "reference":
@@ -664,6 +751,16 @@ def main():
 
         if rank == 0:
             print(json.dumps({"workload": "msolve", "n_gpus": world, "data": "synthetic", **res}))
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    if a.workload == "rhmc48":
+        stream = torch.cuda.Stream(device=dev)
+        res = batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream)
+        if rank == 0:
+            print(json.dumps({"workload": "rhmc48", "n_gpus": world, "data": "synthetic", **res}))
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()

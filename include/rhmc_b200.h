@@ -222,6 +222,9 @@ typedef struct {
                              at the start of every trajectory, instead of at every rescaling as the
                              reference does; 2 lambda_max by power iteration, lambda_min = mass^2 (the
                              exact lower bound of M^dag M, no slow lambda_min iteration) */
+    int single_rhs;       /* 1: every pseudofermion of every species in its own multi-shift solve (the
+                             reference's loop over pseudofermions, inverter.cc:164); 0: all of them
+                             batched into one solve (one link read serves every right-hand side) */
 } rhmc_driver_params;
 
 /* Configures the driver of lib/Update (update.cc, ipdot.cc, momenta.cc, MD_integrators).

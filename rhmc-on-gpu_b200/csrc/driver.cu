@@ -133,8 +133,18 @@ static int solve(rhmc_ctx *c, int s, const Approx &ap, double res, int mode, int
     mp.max_iter = d->P.max_cg;
     mp.mode = mode;
     mp.fmt = fmt;
-    d->solves++;
-    return rhmc_msolve(c, &mp, (double *)x, (const double *)b, nullptr);
+    if (!d->P.single_rhs) {
+        d->solves++;
+        return rhmc_msolve(c, &mp, (double *)x, (const double *)b, nullptr);
+    }
+    mp.nrhs = 1;
+    for (int ps = 0; ps < d->sp[s].no_ps; ps++) {
+        d->solves++;
+        const int rc = rhmc_msolve(c, &mp, (double *)(x + (size_t)ps * ap.order * SP(c)), (const double *)(b + (size_t)ps * SP(c)),
+                                   nullptr);
+        if (rc) return rc;
+    }
+    return RHMC_OK;
 }
 
 // Every pseudofermion of every species solved against its pole set: (M^dag M(m_s) + b_{s,i}) x =
@@ -167,7 +177,7 @@ static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res
     }
     int rc = field(c, "drv_x", xtot, &out.x);
     if (rc) return rc;
-    if (ns == 1 || !same) {
+    if (ns == 1 || !same || d->P.single_rhs) {
         for (int s = 0; s < ns; s++) {
             double2 *in = nullptr;
             rc = field(c, fname(in_base, s), d->sp[s].no_ps, &in);
@@ -548,6 +558,7 @@ int rhmc_driver_setup(rhmc_ctx *c, const rhmc_driver_params *p)
         return fail(RHMC_ERR_ARG, "no_ps, no_flavours, no_md, gauge_scale and max_cg must be positive");
     if (p->integrator < 0 || p->integrator > RHMC_INT_LEAPFROG) return fail(RHMC_ERR_ARG, "unknown integrator");
     if (p->auto_bounds < 0 || p->auto_bounds > 2) return fail(RHMC_ERR_ARG, "auto_bounds must be 0, 1 or 2");
+    if (p->single_rhs != 0 && p->single_rhs != 1) return fail(RHMC_ERR_ARG, "single_rhs must be 0 or 1");
     Driver *d = ensure_driver(c);
     d->P = *p;
     d->sp[0].no_flavours = p->no_flavours;

@@ -84,3 +84,43 @@ def test_species_errors():
         light.add_species(0.05, 1, 1)  # below the context mass
     with pytest.raises(rb.RhmcError):
         both.select_species(2)
+
+
+def test_single_rhs_matches_batched():
+    """The driver's single_rhs option (every pseudofermion in its own solve, as the reference's
+    loop over pseudofermions) and the default batched solve give the same heatbath, action and
+    force: in FP64 mode each right-hand side of a batched solve follows its own recurrences with
+    launch-shape-independent reductions."""
+    g, cf = _data()
+    m = float(g["mass"])
+    dims = tuple(g["dims"])
+    b_l = tuple(g["bounds"])
+    b_s = tuple(np.array(b_l) + M_S ** 2 - m ** 2)
+    phis = [F.random_spinor(dims, seed=2005, n=2), F.random_spinor(dims, seed=2006, n=2)]
+    out = []
+    for single in (0, 1):
+        from gpu_util import new_ctx
+        ctx = new_ctx(dims, mass=m, beta=float(g["beta"]))
+        ctx.set_gauge(g["u"])
+        ctx.driver_setup(no_flavours=2, no_ps=2, residue_md=1e-12, residue_metro=1e-12, single_rhs=single)
+        assert ctx.add_species(M_S, 1, 2) == 1
+        for s, b in enumerate((b_l, b_s)):
+            ctx.select_species(s)
+            for w, c in enumerate(cf):
+                ctx.set_approx(w, c)
+            ctx.set_eig_bounds(*b)
+            ctx.set_phi(phis[s])
+        ctx.first_inv_approx_calc(1e-12)
+        chis = []
+        for s in range(2):
+            ctx.select_species(s)
+            chis.append(ctx.get_chi())
+        ctx.select_species(0)
+        act = ctx.fermion_action()
+        ctx.calc_ipdot_fermion()
+        out.append((chis, act, ctx.get_ipdot()))
+    (c0, a0, i0), (c1, a1, i1) = out
+    for s in range(2):
+        assert rel_err(c1[s], c0[s]) < 1e-14
+    assert abs(a1 - a0) <= 1e-14 * abs(a0)
+    assert rel_err(i1, i0) < 1e-14
