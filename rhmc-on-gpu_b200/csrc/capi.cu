@@ -72,6 +72,8 @@ int rhmc_create(const rhmc_params *p, rhmc_ctx **out)
     c->launches = 0;
     c->hflags = nullptr;
     c->driver = nullptr;
+    c->dh_ready = false;
+    c->dh_cmp = c->dh_down = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaHostAlloc((void **)&c->hflags, 256, cudaHostAllocDefault);
     c->aux = nullptr;
@@ -108,6 +110,15 @@ int rhmc_destroy(rhmc_ctx *c)
         cudaStreamDestroy(c->aux);
         cudaEventDestroy(c->ev_fork);
         cudaEventDestroy(c->ev_join);
+    }
+    if (c->dh_ready) {
+        cudaStreamDestroy(c->dh_cmp);
+        cudaStreamDestroy(c->dh_down);
+        for (int i = 0; i < RHMC_DH_MAXCH; i++) {
+            cudaEventDestroy(c->dh_up_ev[i]);
+            cudaEventDestroy(c->dh_cmp_ev[i]);
+        }
+        cudaEventDestroy(c->dh_done);
     }
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -261,21 +272,90 @@ int rhmc_dslash_repeat(rhmc_ctx *c, int fmt, void *even, void *odd, int n, int r
     return RHMC_OK;
 }
 
+}  // extern "C"
+
+// The device address of host range [p, p + bytes) when it is page-locked memory mapped for the
+// device at both ends (cudaHostAlloc / cudaHostRegister, any runtime of the process), else null.
+static void *mapped_host(void *p, size_t bytes)
+{
+    cudaPointerAttributes a0, a1;
+    if (cudaPointerGetAttributes(&a0, p) != cudaSuccess || cudaPointerGetAttributes(&a1, (char *)p + bytes - 1) != cudaSuccess) {
+        cudaGetLastError();  // clear the sticky-free error of an unregistered pointer
+        return nullptr;
+    }
+    if (a0.type != cudaMemoryTypeHost || a1.type != cudaMemoryTypeHost || !a0.devicePointer || !a1.devicePointer) return nullptr;
+    if ((char *)a1.devicePointer - (char *)a0.devicePointer != (ptrdiff_t)(bytes - 1)) return nullptr;
+    return a0.devicePointer;
+}
+
+extern "C" {
+
 int rhmc_dslash_host(rhmc_ctx *c, int parity_out, double *out, const double *in)
 {
     if (!c || !out || !in || (parity_out != 0 && parity_out != 1)) return fail(RHMC_ERR_ARG, "bad argument");
     const size_t bytes = (size_t)c->Vh * 6 * sizeof(double);
-    void *din, *dout, *iin, *iout;
+    void *din, *dout;  // device copies in the host layout
     CK(c->ws.get("dh_in", bytes, &din));
     CK(c->ws.get("dh_out", bytes, &dout));
-    CK(c->ws.get("dh_iin", bytes, &iin));
-    CK(c->ws.get("dh_iout", bytes, &iout));
-    CK(cudaMemcpyAsync(din, in, bytes, cudaMemcpyHostToDevice, c->stream));
-    launch_spinor_to_internal(c, RHMC_LINKS_F64_18, iin, (const double *)din, 1);
-    cudaError_t e = launch_dslash(c, RHMC_LINKS_F64_18, parity_out, iout, iin, 3 * (size_t)c->Vh, 1, nullptr, 0.0, 0.5, nullptr, nullptr);
-    if (e != cudaSuccess) return cuda_fail(e, "rhmc_dslash_host");
-    launch_spinor_from_internal(c, RHMC_LINKS_F64_18, (double *)dout, iout, 1);
-    CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+    // Chunks of whole t-slabs (half index k runs t-slowest, so a slab is a contiguous range of k
+    // and of the host array): the output of chunk j needs the input of chunks j-1, j, j+1.
+    int nch = 0;
+    for (int n = RHMC_DH_MAXCH; n >= 3; n--)
+        if (c->g.nt % n == 0) { nch = n; break; }
+    if (nch == 0) {  // too few time slices to pipeline: upload, Dslash, download
+        CK(cudaMemcpyAsync(din, in, bytes, cudaMemcpyHostToDevice, c->stream));
+        CK(launch_dslash_f64_range(c, c->stream, parity_out, dout, din, 0, (int)c->Vh));
+        CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return RHMC_OK;
+    }
+    if (!c->dh_ready) {
+        CK(cudaStreamCreateWithFlags(&c->dh_cmp, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->dh_down, cudaStreamNonBlocking));
+        for (int i = 0; i < RHMC_DH_MAXCH; i++) {
+            CK(cudaEventCreateWithFlags(&c->dh_up_ev[i], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->dh_cmp_ev[i], cudaEventDisableTiming));
+        }
+        CK(cudaEventCreateWithFlags(&c->dh_done, cudaEventDisableTiming));
+        c->dh_ready = true;
+    }
+    // The library stream uploads chunk by chunk; the compute stream runs the Dslash of chunk j
+    // once chunk j+1 is in.  When `out` is page-locked host memory (both ends of the range mapped
+    // for the device), the Dslash stores each finished chunk straight into it over PCIe;
+    // otherwise the download stream copies each finished chunk out.  Chunks 0 and nch-1 wrap
+    // around in t, so they are computed last.  Uploads and the output traffic use opposite PCIe
+    // directions and overlap each other and the kernels.
+    const long cs = c->Vh / nch;  // sites per chunk
+    const size_t cb = (size_t)cs * 6 * sizeof(double);
+    double2 *hin = (double2 *)din, *hout = (double2 *)dout;
+    double2 *zout = (double2 *)mapped_host(out, bytes);  // device address of out, or null
+    auto upload = [&](int i) -> int {
+        CK(cudaMemcpyAsync(hin + (size_t)i * cs * 3, in + (size_t)i * cs * 6, cb, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaEventRecord(c->dh_up_ev[i], c->stream));
+        return RHMC_OK;
+    };
+    // the Dslash reads and writes the host layout directly (no conversion kernels)
+    auto compute = [&](int j, int wait_for) -> int {
+        CK(cudaStreamWaitEvent(c->dh_cmp, c->dh_up_ev[wait_for], 0));
+        if (zout) {
+            CK(launch_dslash_f64_range(c, c->dh_cmp, parity_out, zout, hin, (int)(j * cs), (int)cs));
+            return RHMC_OK;
+        }
+        CK(launch_dslash_f64_range(c, c->dh_cmp, parity_out, hout, hin, (int)(j * cs), (int)cs));
+        CK(cudaEventRecord(c->dh_cmp_ev[j], c->dh_cmp));
+        CK(cudaStreamWaitEvent(c->dh_down, c->dh_cmp_ev[j], 0));
+        CK(cudaMemcpyAsync(out + (size_t)j * cs * 6, hout + (size_t)j * cs * 3, cb, cudaMemcpyDeviceToHost, c->dh_down));
+        return RHMC_OK;
+    };
+    int rc;
+    for (int i = 0; i < nch; i++) {
+        if ((rc = upload(i))) return rc;
+        if (i >= 2 && (rc = compute(i - 1, i))) return rc;  // chunk i-1 needs chunks i-2 .. i
+    }
+    // the wrapping chunks: nch-1 needs 0 and nch-2; 0 needs nch-1 and 1 (all uploaded by now)
+    if ((rc = compute(nch - 1, nch - 1)) || (rc = compute(0, nch - 1))) return rc;
+    CK(cudaEventRecord(c->dh_done, zout ? c->dh_cmp : c->dh_down));
+    CK(cudaStreamWaitEvent(c->stream, c->dh_done, 0));
     CK(cudaStreamSynchronize(c->stream));
     return RHMC_OK;
 }

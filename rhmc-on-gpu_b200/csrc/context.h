@@ -84,6 +84,8 @@ inline std::string key_bytes(const K &k) { return std::string(reinterpret_cast<c
 
 }  // namespace rhmc
 
+constexpr int RHMC_DH_MAXCH = 16;  // chunks of the pipelined host-buffer Dslash
+
 struct rhmc_ctx {
     rhmc::Geom g;
     long V, Vh;
@@ -110,6 +112,10 @@ struct rhmc_ctx {
     long launches;  // kernels launched by this context (counted by the host wrappers)
     rhmc::GraphCache graphs;  // instantiated solver-loop graphs
     rhmc::Driver *driver;  // molecular-dynamics driver state (rhmc_driver_setup), or null
+    // pipelined host-buffer Dslash: compute and download streams, per-chunk events (made on first use)
+    cudaStream_t dh_cmp, dh_down;
+    cudaEvent_t dh_up_ev[RHMC_DH_MAXCH], dh_cmp_ev[RHMC_DH_MAXCH], dh_done;
+    bool dh_ready;
 };
 
 namespace rhmc {

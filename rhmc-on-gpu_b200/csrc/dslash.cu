@@ -33,6 +33,8 @@ static void run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in,
     a.stop = nullptr;
     a.stop_set = nullptr;
     a.run_if = nullptr;
+    a.k_lo = 0;
+    a.k_count = 0;
     constexpr int B = DslashCfg<LF, NR, false>::block;
     const int grid = grid_for(c->Vh, B);
     if (y) dslash_kernel<LF, NR, true, false, NoFin><<<grid, B, 0, c->stream>>>(a);
@@ -62,6 +64,34 @@ static void run_n(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *i
         }
     }
     }
+}
+
+// FP64 18-real half-Dslash of one spinor in the reference's site-major layout (A64S) onto the
+// output sites [k_lo, k_lo + k_count) only, on stream s (the host-buffer entry point pipelines
+// its copies against these slabs)
+cudaError_t launch_dslash_f64_range(rhmc_ctx *c, cudaStream_t s, int p_out, void *out, const void *in, int k_lo, int k_count)
+{
+    L64_18 l18;
+    cudaError_t e = links_f64_18(c, &l18);
+    if (e != cudaSuccess) return e;
+    L64_18A lf;
+    lf.p = l18.p;
+    lf.Vh = l18.Vh;
+    DslashArgs<L64_18A, 1> a;
+    memset(&a, 0, sizeof(a));
+    a.g = c->g;
+    a.p_out = p_out;
+    a.links = lf;
+    a.in = (const double2 *)in;
+    a.out = (double2 *)out;
+    a.stride = 3 * (size_t)c->Vh;
+    a.beta = 0.5;
+    a.k_lo = k_lo;
+    a.k_count = k_count;
+    constexpr int B = DslashCfg<L64_18, 1, false>::block;
+    dslash_kernel<L64_18A, 1, false, false, NoFin><<<grid_for(k_count, B), B, 0, s>>>(a);
+    c->launches++;
+    return cudaGetLastError();
 }
 
 cudaError_t launch_dslash(rhmc_ctx *c, int fmt, int p_out, void *out, const void *in, size_t stride, int n,

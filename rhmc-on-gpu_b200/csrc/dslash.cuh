@@ -55,6 +55,7 @@ struct DslashArgs {
     const int *stop;    // optional: skip the launch when *stop != 0 ...
     int *stop_set;      // ... and then set *stop_set = 1 (solver loop control)
     const int *run_if;  // optional: skip the launch when *run_if == 0
+    int k_lo, k_count;  // output sites [k_lo, k_lo + k_count) (k_count 0: all Vh); no RED with a range
 };
 
 template <class LF, int NR, bool HAS_Y, bool RED, class FIN, int BLOCK = DslashCfg<LF, NR, RED>::block,
@@ -67,15 +68,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
         return;
     }
     if (a.run_if && *(volatile const int *)a.run_if == 0) return;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = a.k_lo + blockIdx.x * blockDim.x + threadIdx.x;
     const int Vh = a.g.Vh;
+    const int kend = a.k_count ? a.k_lo + a.k_count : Vh;
     // y (read only by the epilogue) is fetched into shared memory by cp.async at the start, so its
     // DRAM latency overlaps the stencil instead of following it (when the block's copy fits)
     typedef typename LF::store S;
     typedef typename S::elem E;
-    constexpr bool PF = HAS_Y && (NR * S::planes * BLOCK * sizeof(E) <= 24576);
+    constexpr bool PF = HAS_Y && S::soa && (NR * S::planes * BLOCK * sizeof(E) <= 24576);
     __shared__ __align__(16) E ysm[PF ? NR * S::planes * BLOCK : 1];
-    if (PF && k < Vh) {
+    if (PF && k < kend) {
 #pragma unroll
         for (int r = 0; r < NR; r++)
 #pragma unroll
@@ -88,7 +90,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
 #pragma unroll
     for (int j = 0; j < NR; j++) red[j] = 0.0;
 
-    if (k < Vh) {
+    if (k < kend) {
         const Site s = site_of(a.g, a.p_out, k);
         vec3<R> acc[NR];
 #pragma unroll

@@ -14,6 +14,7 @@ void launch_algebra_from_ref(rhmc_ctx *c, double *A, const double *ref, int anti
 void launch_algebra_to_ref(rhmc_ctx *c, double *ref, const double *A, int antiherm);
 void launch_spinor_to_internal(rhmc_ctx *c, int fmt, void *dst, const double *src, int n);
 void launch_spinor_from_internal(rhmc_ctx *c, int fmt, double *dst, const void *src, int n);
+cudaError_t launch_dslash_f64_range(rhmc_ctx *c, cudaStream_t s, int p_out, void *out, const void *in, int k_lo, int k_count);
 
 // Largest number of right-hand sides one Dslash launch carries.
 constexpr int DSLASH_MAX_NR = 8;

@@ -128,6 +128,7 @@ __device__ __forceinline__ void reconstruct_row2(su3m<R> &u, R eta)
 struct F64S;
 struct F32S;
 struct H16S;
+struct A64S;
 
 // FP64, 18 reals: 9 double2 planes
 struct L64_18 {
@@ -147,6 +148,11 @@ struct L64_18 {
             u.e[e / 3][e % 3] = mk<double>(v.x, v.y);
         }
     }
+};
+
+// FP64 18-real links with spinors in the reference's site-major host layout (A64S)
+struct L64_18A : L64_18 {
+    typedef A64S store;
 };
 
 // FP64, 12 reals: 6 double2 planes, row 2 reconstructed
@@ -278,6 +284,7 @@ struct F64S {
     typedef double real;
     typedef double2 elem;
     static constexpr int planes = 3;
+    static constexpr bool soa = true;  // plane c of site k at c * Vh + k
     template <typename R>
     __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int Vh, int k)
     {
@@ -313,6 +320,7 @@ struct F32S {
     typedef float real;
     typedef float2 elem;
     static constexpr int planes = 3;
+    static constexpr bool soa = true;
     template <typename R>
     __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int Vh, int k)
     {
@@ -343,6 +351,44 @@ struct F32S {
     }
 };
 
+// The reference's host layout (Vec3 arrays, lib/Tools/vec3.h): the 3 complex numbers of a site
+// consecutive, sites in half-index order.  A warp's 32 sites are 1536 contiguous bytes, so its
+// loads stay coalesced; the host-buffer Dslash reads and writes it without conversion kernels.
+struct A64S {
+    typedef double real;
+    typedef double2 elem;
+    static constexpr int planes = 3;
+    static constexpr bool soa = false;
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int, int k)
+    {
+        vec3<R> r;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const elem a = __ldg(v + (size_t)3 * k + c);
+            r.c[c] = mk<R>((R)a.x, (R)a.y);
+        }
+        return r;
+    }
+    template <typename R>
+    __device__ __forceinline__ static void store(elem *v, int, int k, const vec3<R> &r)
+    {
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[(size_t)3 * k + c] = make_double2((double)r.c[c].re, (double)r.c[c].im);
+    }
+    template <typename R>
+    __device__ __forceinline__ static vec3<R> load_plain(const elem *v, int, int k)
+    {
+        vec3<R> r;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const elem a = v[3 * k + c];
+            r.c[c] = mk<R>((R)a.x, (R)a.y);
+        }
+        return r;
+    }
+};
+
 // Half precision with a per-site scale, one 16-byte vector per site: words x, y, z hold the
 // three colour components as __half2 divided by the site's largest |real or imaginary part|,
 // word w holds that scale as a float (16 bytes per site instead of 24 in FP32, and one load
@@ -351,6 +397,7 @@ struct H16S {
     typedef float real;
     typedef uint4 elem;
     static constexpr int planes = 1;
+    static constexpr bool soa = true;
     __device__ __forceinline__ static float2 h2f(unsigned w) { return __half22float2(*reinterpret_cast<const __half2 *>(&w)); }
     __device__ __forceinline__ static unsigned f2h(float a, float b)
     {

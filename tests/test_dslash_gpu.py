@@ -92,9 +92,11 @@ def test_mdagm_vs_oracle(oracle_mod):
         assert rel_err(got, ref) < 1e-13
 
 
-def test_dslash_host_reference_facing(oracle_mod):
+@pytest.mark.parametrize("dims", [(4, 4, 4, 4), (4, 6, 2, 10), (4, 4, 4, 2), (8, 8, 8, 16)])
+def test_dslash_host_reference_facing(oracle_mod, dims):
+    """Host arrays in the reference's layout: uploaded, applied and downloaded in chunks of
+    t-slabs (4, 5 and 8 chunks here; nt = 2 has too few slabs and runs unchunked)."""
     from gpu_util import new_ctx
-    dims = (4, 4, 4, 4)
     ctx = new_ctx(dims)
     u = F.random_links(dims, seed=21)
     ctx.set_gauge(u)
@@ -105,6 +107,16 @@ def test_dslash_host_reference_facing(oracle_mod):
     assert rel_err(out, orc.doe(u, x)) < 1e-13
     ctx.dslash_host(0, out, x)
     assert rel_err(out, orc.deo(u, x)) < 1e-13
+    # page-locked buffers: the output is stored into host memory by the kernels themselves
+    import torch
+    pin_in = torch.from_numpy(np.ascontiguousarray(x).view(np.float64).reshape(-1).copy()).pin_memory()
+    pin_out = torch.zeros(pin_in.numel(), dtype=torch.float64).pin_memory()
+    ctx.dslash_host(1, pin_out.numpy(), pin_in.numpy())
+    got = pin_out.numpy().view(np.complex128).reshape(x.shape)
+    assert rel_err(got, orc.doe(u, x)) < 1e-13
+    ctx.dslash_host(0, pin_out.numpy(), pin_in.numpy())
+    got = pin_out.numpy().view(np.complex128).reshape(x.shape)
+    assert rel_err(got, orc.deo(u, x)) < 1e-13
 
 
 def test_gauge_roundtrip_exact():
