@@ -107,8 +107,10 @@ int rhmc_dslash(rhmc_ctx *ctx, int fmt, int parity_out, void *out, const void *i
 /* `repeats` times: odd = D_oe even, then even = D_eo odd (n RHS), issued back to back from C
  * so that timing loops measure the kernels and not the caller's launch overhead. */
 int rhmc_dslash_repeat(rhmc_ctx *ctx, int fmt, void *even, void *odd, int n, int repeats);
-/* Reference-facing form of Deo/Doe: host spinors in the reference layout, FP64 links.
- * Copies in, applies, copies out (used for the end-to-end measurement). */
+/* Reference-facing form of Deo/Doe (lib/Action/fermionmatrix.cc:8-97): host spinors in the
+ * reference layout (Vec3[Vh]), FP64 links; blocking.  The input is uploaded in chunks of
+ * t-slabs that the Dslash consumes as they arrive; a page-locked `out` is written by the kernel
+ * directly, any other `out` through a copy per chunk. */
 int rhmc_dslash_host(rhmc_ctx *ctx, int parity_out, double *out, const double *in);
 /* out = (M^dag M + shift) in on even sites = (mass^2 + shift) in - Deo Doe in
  * (lib/Action/Inverter/inverter.cc:3, 206-216); internal-layout device spinors. */
