@@ -400,6 +400,17 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
                                         4 * V * (144 + 128) + -(-nv // 8) * 4 * V * 144 + nv * (Vh * 96 + V * 48))
     kern["mom_update"] = (_timed(torch, stream, lambda: ctx.mom_update(0.0), reps), 4 * V * 3 * 64)
     kern["link_update"] = (_timed(torch, stream, lambda: ctx.link_update(0.0), reps), 4 * V * (64 + 2 * 144))
+    # rational sum chi = a0 b + sum_i a_i x_i over one pole set (15 shifted vectors)
+    chi_out = torch.zeros(6 * Vh, dtype=torch.float64, device=dev)
+    kern["rational_sum_15_poles"] = (_timed(torch, stream, lambda: ctx.rational_sum(chi_out, xk, xk[:6 * Vh], 0.5,
+                                                                                    coef[:NF_DEG]), reps),
+                                     (NF_DEG + 2) * Vh * 48)
+    # actions and plaquette: one pass over the links (or momenta) and an FP64 reduction; these
+    # return host values, so the time includes the synchronisation and the read-back
+    kern["gauge_action"] = (_timed(torch, stream, lambda: ctx.gauge_action(), reps), 4 * V * 144)
+    kern["plaquette"] = (_timed(torch, stream, lambda: ctx.plaquette(), reps), 4 * V * 144)
+    kern["momentum_action"] = (_timed(torch, stream, lambda: ctx.momentum_action(), reps), 4 * V * 64)
+    del chi_out
     peak, _ = load_peaks()
     fp64_peak = ctx.fma_peak(True)
     out["kernels"] = {k: {"ms": round(t, 4), "alg_bytes": b, "gbs": round(b / (t * 1e-3) / 1e9, 1),

@@ -65,25 +65,28 @@ __global__ void __launch_bounds__(UPD_BLOCK) link_update_kernel(Geom g, double2 
     store_link64(U, Vh, mu, p, k, u);
 }
 
-// per site (both parities): temporal and spatial sums of ReTr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag)
+// temporal and spatial sums of ReTr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag): one thread per
+// site (both parities) and pair of planes, {(0,1),(2,3)}, {(0,2),(1,3)} or {(0,3),(1,2)} (two
+// plaquettes each, every link direction used twice), with the pair as the fastest block index
+// so that the three threads of a site range run together and share its links in L2.
 __global__ void __launch_bounds__(UPD_BLOCK) plaq_kernel(Geom g, const double2 *__restrict__ U, double *partials)
 {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pair = blockIdx.x % 3;
+    const long t = (long)(blockIdx.x / 3) * blockDim.x + threadIdx.x;
     const int Vh = g.Vh;
     double v[2] = {0.0, 0.0};
     if (t < 2L * Vh) {
         const int p = t >= Vh, q = 1 - p;
         const int k = (int)(t - (long)p * Vh);
         const Site s = site_of(g, p, k);
-        for (int mu = 0; mu < 3; mu++) {
-            const M3 umu = load_link64(U, Vh, mu, p, k);
-            const int kpm = neighbour(g, s, mu, +1);
-            for (int nu = mu + 1; nu < 4; nu++) {
-                M3 a = m3_mul(umu, load_link64(U, Vh, nu, q, kpm));
-                a = m3_mul_nd(a, load_link64(U, Vh, mu, q, neighbour(g, s, nu, +1)));
-                a = m3_mul_nd(a, load_link64(U, Vh, nu, p, k));
-                v[nu == 3 ? 0 : 1] += m3_retr(a);
-            }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int mu = h == 0 ? 0 : (pair == 0 ? 2 : 1);
+            const int nu = h == 0 ? pair + 1 : (pair == 2 ? 2 : 3);
+            M3 a = m3_mul(load_link64(U, Vh, mu, p, k), load_link64(U, Vh, nu, q, neighbour(g, s, mu, +1)));
+            a = m3_mul_nd(a, load_link64(U, Vh, mu, q, neighbour(g, s, nu, +1)));
+            a = m3_mul_nd(a, load_link64(U, Vh, nu, p, k));
+            v[nu == 3 ? 0 : 1] += m3_retr(a);
         }
     }
     __shared__ double smem[2 * 32];
@@ -174,7 +177,7 @@ int link_update(rhmc_ctx *c, double step)
 // sums over all sites of ReTr(plaquette): temporal (nu = 3) and spatial
 int plaquette_sums(rhmc_ctx *c, double *temporal, double *spatial)
 {
-    const int nb = grid_for(2L * c->Vh, UPD_BLOCK);
+    const int nb = 3 * grid_for(2L * c->Vh, UPD_BLOCK);  // 3 pairs of planes per site range
     void *part;
     CK(c->ws.get("red_part", (size_t)nb * 2 * sizeof(double), &part));
     plaq_kernel<<<nb, UPD_BLOCK, 0, c->stream>>>(c->g, c->U64, (double *)part);
