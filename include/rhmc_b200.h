@@ -196,6 +196,31 @@ int rhmc_gauge_action(rhmc_ctx *ctx, double *out);
 int rhmc_momentum_action(rhmc_ctx *ctx, double *out);
 /* spatial and temporal plaquette as Conf::calc_plaq (lib/Measurements/gaugemeas.cc:7-65). */
 int rhmc_plaquette(rhmc_ctx *ctx, double *spatial, double *temporal);
+/* Polyakov loop as Conf::calc_poly (lib/Measurements/gaugemeas.cc:66-106): the average over spatial
+ * points of -Tr/3 of the ordered product of the temporal links (the minus sign undoes the
+ * antiperiodic phase folded into them). */
+int rhmc_polyakov(rhmc_ctx *ctx, double *re, double *im);
+/* chiral_meas (lib/Measurements/chiralmeas.cc:18-194, without imaginary chemical potential) for
+ * nrand pairs of noise vectors (even, odd; n consecutive spinors of the reference layout, host or
+ * device per `location`; the reference draws Z2 noise, the caller supplies it here):
+ * phi_e = m rnd_e - Deo rnd_o, (M^dag M) chi_e = phi_e solved in FP64 to the absolute `residual`,
+ * chi_o = (rnd_o - Doe chi_e) / m, then out[8] = chiral condensate, energy, baryon and pressure
+ * densities as (re, im) pairs, averaged over the noise pairs. */
+int rhmc_chiral_meas(rhmc_ctx *ctx, int nrand, int no_flavours, const double *noise_e, const double *noise_o, double residual,
+                     int max_iter, int location, double *out);
+
+/* ------------------------------------------------------------------ configuration files */
+/* The reference's text configuration (Conf::write_last, lib/Main/Conf/conf.cc:175-200): a header
+ * "nx ny nz nt beta mass no_flavours update_iteration" (beta and mass of the context), then every
+ * link of the current gauge field (eta folded in) as 3 rows of "(re,im)" numbers, 16 digits. */
+int rhmc_write_conf(rhmc_ctx *ctx, const char *path, int no_flavours, long update_iteration);
+/* Reads such a file into the gauge field (the stored-conf start of Conf::Conf, conf.cc:55-94);
+ * fails on a lattice-size mismatch.  reunitarize = 1 applies the reunitarisation with eta that
+ * the reference's reader means to apply but does not (its calls act on u_work before u_work is
+ * overwritten); 0 keeps the stored numbers as the reference does.  Header values are returned
+ * through the non-null pointers. */
+int rhmc_read_conf(rhmc_ctx *ctx, const char *path, int reunitarize, double *beta, double *mass, int *no_flavours,
+                   long *update_iteration);
 /* sum over n internal FP64 spinors of Re<a, b> (fermion_action, lib/Action/action.cc:65-107). */
 int rhmc_rdot(rhmc_ctx *ctx, const double *a, const double *b, int n, double *out);
 /* out_r = a0 b_r + sum_i a_i x_{r,i} (rationalapprox.cc:300-311; cuda_sol_sum, lib/Cuda/cuda_sol_sum.cu:168-221);

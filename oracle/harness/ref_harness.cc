@@ -27,6 +27,8 @@
 #include "lib/Tools/RationalApprox/rationalapprox.h"
 #include "lib/Action/Findminmax/findminmax.h"
 
+void chiral_meas(complex<REAL> &chiral, complex<REAL> &e_dens, complex<REAL> &b_dens, complex<REAL> &p_dens);
+
 #include <cstring>
 
 static double h_min = 1.0e-3, h_max = 64.0;
@@ -226,6 +228,12 @@ void ref_setup(unsigned long seed)
     fermion_shiftmulti = new ShiftMultiFermion;
     h_in = new Fermion;
     h_out = new Fermion;
+    chi_e = new Fermion;  // the measurement fields (lib/Main/init.cc:71-76)
+    chi_o = new Fermion;
+    phi_e = new Fermion;
+    phi_o = new Fermion;
+    rnd_e = new Fermion;
+    rnd_o = new Fermion;
     first_inv_approx_norm_coeff = new RationalApprox;
     md_inv_approx_norm_coeff = new RationalApprox;
     last_inv_approx_norm_coeff = new RationalApprox;
@@ -355,6 +363,46 @@ double ref_action_end(void)
     calc_action(plaq_test, -1);
     global_sum(plaq_test, size);
     return -plaq_test[0];
+}
+
+// Conf::calc_poly (lib/Measurements/gaugemeas.cc:66-106) measures u_save; saved first.
+void ref_polyakov(double *re, double *im)
+{
+    gauge_conf->save();
+    REAL r, i;
+    gauge_conf->calc_poly(r, i);
+    *re = r;
+    *im = i;
+}
+
+// chiral_meas (lib/Measurements/chiralmeas.cc:18-194) draws its own Z2 noise (rand_vect = 1) and
+// solves with the CPU CG; the noise it used is copied out afterwards so that the CUDA path can be
+// given the same vectors.  out: chiral, energy, baryon and pressure densities as (re, im).
+void ref_chiral_meas(double *out, double *noise_e, double *noise_o)
+{
+    complex<REAL> ch, ed, bd, pd;
+    chiral_meas(ch, ed, bd, pd);
+    out[0] = real(ch); out[1] = imag(ch);
+    out[2] = real(ed); out[3] = imag(ed);
+    out[4] = real(bd); out[5] = imag(bd);
+    out[6] = real(pd); out[7] = imag(pd);
+    smartpack_fermion_d(reinterpret_cast<float *>(noise_e), rnd_e);
+    smartpack_fermion_d(reinterpret_cast<float *>(noise_o), rnd_o);
+}
+
+// Conf::write_last (lib/Main/Conf/conf.cc:175-200) into ./config, and the stored-conf start of
+// Conf::Conf (conf.cc:55-94) from ./config, whose links are copied out exactly.
+void ref_write_conf(void)
+{
+    gauge_conf->save();
+    gauge_conf->write_last();
+}
+
+void ref_read_conf(double *u)
+{
+    Conf *t = new Conf(2);
+    smartpack_gauge(reinterpret_cast<float *>(u), t);
+    delete t;
 }
 
 // Conf::calc_plaq measures u_save; the harness saves u_work first.

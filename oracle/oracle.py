@@ -58,6 +58,9 @@ class Oracle:
         L.orc_mdagm.argtypes = [_D, _D, _D, ctypes.c_double, ctypes.c_double]
         L.orc_msolve.argtypes = [_D, _D, _D, ctypes.c_double, ctypes.c_int, _D, ctypes.c_double, ctypes.c_int]
         L.orc_msolve.restype = ctypes.c_int
+        L.orc_polyakov.argtypes = [_D, _D, _D]
+        L.orc_chiral_meas.argtypes = [_D, _D, _D, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, _D]
+        L.orc_chiral_meas.restype = ctypes.c_int
         L.orc_rational_sum.argtypes = [_D, _D, _D, ctypes.c_double, _D, ctypes.c_int]
         L.orc_fermion_force_accum.argtypes = [_D, _D, _D, _D, ctypes.c_int]
         L.orc_staples.argtypes = [_D, _D]
@@ -227,6 +230,21 @@ class Oracle:
     def rdot(self, a, b):
         return self.lib.orc_rdot(_dp(np.ascontiguousarray(a)), _dp(np.ascontiguousarray(b)))
 
+    def polyakov(self, u):
+        """Conf::calc_poly (lib/Measurements/gaugemeas.cc:66-106): (re, im)."""
+        re, im = np.zeros(1), np.zeros(1)
+        self.lib.orc_polyakov(_dp(np.ascontiguousarray(u, np.complex128)), _dp(re), _dp(im))
+        return float(re[0]), float(im[0])
+
+    def chiral_meas(self, u, noise_e, noise_o, mass, no_flavours, res, max_cg=100000):
+        """chiral_meas for one pair of noise vectors (lib/Measurements/chiralmeas.cc:44-183):
+        chiral condensate, energy, baryon and pressure densities as 4 complex numbers."""
+        out = np.zeros(8)
+        self.lib.orc_chiral_meas(_dp(np.ascontiguousarray(u, np.complex128)),
+                                 _dp(np.ascontiguousarray(noise_e, np.complex128)),
+                                 _dp(np.ascontiguousarray(noise_o, np.complex128)), mass, no_flavours, res, max_cg, _dp(out))
+        return out[0::2] + 1j * out[1::2]
+
     def plaquette(self, u):
         s = np.zeros(1)
         t = np.zeros(1)
@@ -271,6 +289,9 @@ class RefLib:
         L.ref_link_update.argtypes = [ctypes.c_double]
         L.ref_action_end.restype = ctypes.c_double
         L.ref_plaquette.argtypes = [_D, _D]
+        L.ref_polyakov.argtypes = [_D, _D]
+        L.ref_chiral_meas.argtypes = [_D, _D, _D]
+        L.ref_read_conf.argtypes = [_D]
         L.ref_trajectory.argtypes = [ctypes.c_int, ctypes.c_double, _I]
         L.ref_trajectory.restype = ctypes.c_double
         L.ref_setup(seed)
@@ -423,6 +444,51 @@ class RefLib:
         t = np.zeros(1)
         self.lib.ref_plaquette(_dp(s), _dp(t))
         return float(s[0]), float(t[0])
+
+    def write_conf(self, directory):
+        """Conf::write_last of the current links into <directory>/config; returns its text."""
+        cwd = os.getcwd()
+        try:
+            os.chdir(directory)
+            self.lib.ref_write_conf()
+            with open("config", "rb") as f:
+                return f.read()
+        finally:
+            os.chdir(cwd)
+
+    def read_conf(self, directory):
+        """The links the reference's stored-conf start reads from <directory>/config."""
+        u = np.zeros((4 * self.V, 3, 3), np.complex128)
+        cwd = os.getcwd()
+        try:
+            os.chdir(directory)
+            self.lib.ref_read_conf(_dp(u))
+        finally:
+            os.chdir(cwd)
+        return u
+
+    def param(self, which):
+        """Compile-time parameter of this build: 0 mass, 1 beta, 2 no_flavours, 3 residue_metro,
+        4 residue_md, 5 max_cg."""
+        self.lib.ref_param.restype = ctypes.c_double
+        return float(self.lib.ref_param(which))
+
+    def polyakov(self):
+        """Conf::calc_poly (lib/Measurements/gaugemeas.cc:66-106) of the current links: (re, im)."""
+        r = np.zeros(1)
+        i = np.zeros(1)
+        self.lib.ref_polyakov(_dp(r), _dp(i))
+        return float(r[0]), float(i[0])
+
+    def chiral_meas(self):
+        """chiral_meas (lib/Measurements/chiralmeas.cc:18-194) with the reference's own Z2 noise and
+        CPU CG: returns the 4 complex results (chiral condensate, energy, baryon and pressure
+        densities) and the even and odd noise vectors it drew, each (Vh, 3) complex."""
+        out = np.zeros(8)
+        ne = np.zeros((self.Vh, 3), np.complex128)
+        no = np.zeros((self.Vh, 3), np.complex128)
+        self.lib.ref_chiral_meas(_dp(out), _dp(ne), _dp(no))
+        return out[0::2] + 1j * out[1::2], ne, no
 
     def trajectory(self, integrator, uniform):
         acc = np.zeros(1, np.int32)

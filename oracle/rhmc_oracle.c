@@ -646,3 +646,102 @@ void orc_plaquette(const double *u_, double *pls, double *plt)
     *pls = d2[0] * inv3 * 0.3333333333333333333333333333333;
     free(d1); free(d2);
 }
+
+/* ---------------------------------------------------------------- measurements */
+/* Conf::calc_poly: lib/Measurements/gaugemeas.cc:66-106.  From each of the reference's sites
+ * r < vol3 (the even sites of the slabs t = 0 and t = 1: one per spatial point) the ordered
+ * product of the nt temporal links; minus sign for the antiperiodic phase folded into them. */
+void orc_polyakov(const double *u_, double *re, double *im)
+{
+    const su3 *u = (const su3 *)u_;
+    long vol3 = (long)g_nx * g_ny * g_nz;
+    double *d1 = (double *)malloc(sizeof(double) * vol3), *d2 = (double *)malloc(sizeof(double) * vol3);
+    for (long r = 0; r < vol3; r++) {
+        su3 aux;
+        su3_one(&aux);
+        long r2 = r;
+        for (int t = 0; t < g_nt; t++) {
+            su3_mulassign(&aux, &u[r2 + 3 * g_V]);
+            r2 = g_nnp[r2 * 4 + 3];
+        }
+        d1[r] = -su3_retr(&aux);
+        d2[r] = -(aux.c[0][0].im + aux.c[1][1].im + aux.c[2][2].im);
+    }
+    global_sum(d1, vol3);
+    global_sum(d2, vol3);
+    const double inv_vol3 = 1.0 / (double)vol3, one_by_three = 1.0 / 3.0;
+    *re = d1[0] * inv_vol3 * one_by_three;
+    *im = d2[0] * inv_vol3 * one_by_three;
+    free(d1); free(d2);
+}
+
+static cplx vec_cscal(const vec3 *a, const vec3 *b)  /* c_scalprod, lib/Tools/vec3.h:227-235 */
+{
+    cplx r = { 0.0, 0.0 };
+    for (int c = 0; c < 3; c++) r = cadd(r, cmul(cconj(a->c[c]), b->c[c]));
+    return r;
+}
+
+/* chiral_meas for one pair of Z2 noise vectors: lib/Measurements/chiralmeas.cc:44-183 (the
+ * branch without imaginary chemical potential).  out: chiral condensate, energy, baryon and
+ * pressure densities as (re, im) pairs.  The even solve is (M^dag M) chi_e = phi_e to the
+ * absolute residual res (the reference's invert, started here from zero). */
+int orc_chiral_meas(const double *u_, const double *ne_, const double *no_, double mass, int nf, double res, int max_cg,
+                    double *out)
+{
+    const su3 *u = (const su3 *)u_;
+    const vec3 *rnd_e = (const vec3 *)ne_, *rnd_o = (const vec3 *)no_;
+    long Vh = g_Vh;
+    vec3 *phi_e = (vec3 *)malloc(sizeof(vec3) * Vh), *chi_e = (vec3 *)malloc(sizeof(vec3) * Vh);
+    vec3 *phi_o = (vec3 *)malloc(sizeof(vec3) * Vh), *chi_o = (vec3 *)malloc(sizeof(vec3) * Vh);
+    double *v[8];
+    for (int j = 0; j < 8; j++) v[j] = (double *)malloc(sizeof(double) * Vh);
+    orc_deo((double *)phi_e, no_, u_);
+    for (long i = 0; i < Vh; i++)
+        for (int c = 0; c < 3; c++) phi_e[i].c[c] = csub(cscal(mass, rnd_e[i].c[c]), phi_e[i].c[c]);
+    const double zero = 0.0;
+    int cg = orc_msolve((double *)chi_e, (const double *)phi_e, u_, mass, 1, &zero, res, max_cg);
+    orc_doe((double *)phi_o, (const double *)chi_e, u_);
+    const double one_by_mass = 1.0 / mass;
+    for (long i = 0; i < Vh; i++)
+        for (int c = 0; c < 3; c++) chi_o[i].c[c] = cscal(one_by_mass, csub(rnd_o[i].c[c], phi_o[i].c[c]));
+    for (long i = 0; i < Vh; i++) {
+        const long j = i + Vh;
+        cplx ch = cadd(vec_cscal(&rnd_o[i], &chi_o[i]), vec_cscal(&rnd_e[i], &chi_e[i]));
+        /* temporal hops: energy (p1 - p2) and baryon (p1 + p2) densities */
+        vec3 ve = su3_mul_vec(&u[i + 3 * g_V], &chi_o[g_nnp[i * 4 + 3] - Vh]);
+        vec3 we = su3_mul_vec(&u[i + 3 * g_V], &rnd_o[g_nnp[i * 4 + 3] - Vh]);
+        cplx p1 = vec_cscal(&rnd_e[i], &ve), p2 = vec_cscal(&we, &chi_e[i]);
+        cplx c1 = csub(p1, p2), c2 = cadd(p1, p2);
+        vec3 vo = su3_mul_vec(&u[j + 3 * g_V], &chi_e[g_nnp[j * 4 + 3]]);
+        vec3 wo = su3_mul_vec(&u[j + 3 * g_V], &rnd_e[g_nnp[j * 4 + 3]]);
+        p1 = vec_cscal(&rnd_o[i], &vo);
+        p2 = vec_cscal(&wo, &chi_o[i]);
+        c1 = cadd(c1, csub(p1, p2));
+        c2 = cadd(c2, cadd(p1, p2));
+        /* spatial hops: pressure density */
+        cplx cp = { 0.0, 0.0 };
+        for (int k = 0; k < 3; k++) {
+            ve = su3_mul_vec(&u[i + k * g_V], &chi_o[g_nnp[i * 4 + k] - Vh]);
+            we = su3_mul_vec(&u[i + k * g_V], &rnd_o[g_nnp[i * 4 + k] - Vh]);
+            cp = cadd(cp, vec_cscal(&rnd_e[i], &ve));
+            cp = csub(cp, vec_cscal(&we, &chi_e[i]));
+            vo = su3_mul_vec(&u[j + k * g_V], &chi_e[g_nnp[j * 4 + k]]);
+            wo = su3_mul_vec(&u[j + k * g_V], &rnd_e[g_nnp[j * 4 + k]]);
+            cp = cadd(cp, vec_cscal(&rnd_o[i], &vo));
+            cp = csub(cp, vec_cscal(&wo, &chi_o[i]));
+        }
+        v[0][i] = ch.re; v[1][i] = ch.im;
+        v[2][i] = c1.re; v[3][i] = c1.im;
+        v[4][i] = c2.re; v[5][i] = c2.im;
+        v[6][i] = cp.re; v[7][i] = cp.im;
+    }
+    const double inv_size = 1.0 / (double)g_V;
+    for (int j = 0; j < 8; j++) {
+        global_sum(v[j], Vh);
+        out[j] = v[j][0] * ((j < 2 ? 1.0 : 0.5) * nf * 0.25 * inv_size);
+        free(v[j]);
+    }
+    free(phi_e); free(chi_e); free(phi_o); free(chi_o);
+    return cg;
+}

@@ -291,6 +291,41 @@ def _plaq(self):
 
 
 Context.plaquette = _plaq
+
+
+def _polyakov(self):
+    re, im = ctypes.c_double(), ctypes.c_double()
+    self.call("rhmc_polyakov", ctypes.byref(re), ctypes.byref(im))
+    return re.value, im.value
+
+
+def _chiral_meas(self, noise_e, noise_o, residual=1e-10, no_flavours=2, max_iter=100000):
+    """chiral_meas for the given noise pairs (host (n, Vh, 3) complex or (Vh, 3)): chiral condensate,
+    energy, baryon and pressure densities as 4 complex numbers."""
+    ne = np.ascontiguousarray(noise_e, np.complex128)
+    no = np.ascontiguousarray(noise_o, np.complex128)
+    n = 1 if ne.ndim == 2 else ne.shape[0]
+    out = np.zeros(8)
+    self.call("rhmc_chiral_meas", n, int(no_flavours), ne, no, float(residual), int(max_iter), HOST, out)
+    return out[0::2] + 1j * out[1::2]
+
+
+def _write_conf(self, path, no_flavours=2, update_iteration=0):
+    self.call("rhmc_write_conf", str(path).encode(), int(no_flavours), ctypes.c_long(update_iteration))
+
+
+def _read_conf(self, path, reunitarize=1):
+    b, m = ctypes.c_double(), ctypes.c_double()
+    nf, it = ctypes.c_int(), ctypes.c_long()
+    self.call("rhmc_read_conf", str(path).encode(), int(reunitarize), ctypes.byref(b), ctypes.byref(m), ctypes.byref(nf),
+              ctypes.byref(it))
+    return {"beta": b.value, "mass": m.value, "no_flavours": nf.value, "update_iteration": it.value}
+
+
+Context.write_conf = _write_conf
+Context.read_conf = _read_conf
+Context.polyakov = _polyakov
+Context.chiral_meas = _chiral_meas
 Context.rational_sum = lambda self, out, x, b, a0, a, nrhs=1: self.call(
     "rhmc_rational_sum", nrhs, len(a), float(a0), np.ascontiguousarray(a, np.float64), x, b, out)
 

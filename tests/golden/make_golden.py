@@ -134,18 +134,56 @@ def make_packer(tag):
     print(tag, "packer fixture written", sorted(out))
 
 
+def make_meas(tag, ncalls=2):
+    """The reference's measurements on the fixture links of ref_<tag>.npz: Conf::calc_poly and
+    ncalls calls of chiral_meas (rand_vect = 1), each with the Z2 noise it drew (copied out of the
+    reference after the call) and its chiral condensate, energy, baryon and pressure densities."""
+    import oracle
+    g = dict(np.load(os.path.join(HERE, "ref_%s.npz" % tag)))
+    ref = oracle.RefLib(tag)
+    ref.set_links(g["u"])
+    out = {"polyakov": np.array(ref.polyakov())}
+    res, ne, no = [], [], []
+    for _ in range(ncalls):
+        r, e, o = ref.chiral_meas()
+        res.append(r)
+        ne.append(e)
+        no.append(o)
+    out["chiral"] = np.array(res)
+    out["noise_e"] = np.array(ne)
+    out["noise_o"] = np.array(no)
+    # the configuration file the reference writes for these links, and what its reader makes of
+    # it (4^4 only, to keep the fixtures small)
+    if tag == "t4":
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            out["conf_text"] = np.frombuffer(ref.write_conf(d), np.uint8)
+            out["conf_read"] = ref.read_conf(d)
+    out["residue_metro"] = np.array(ref.param(3))
+    out["no_flavours"] = np.array(ref.param(2))
+    np.savez_compressed(os.path.join(HERE, "ref_%s_meas.npz" % tag), **out)
+    print(tag, "measurement fixture written", sorted(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--build", action="store_true", help="(re)build the reference harness first")
     ap.add_argument("--packer-only", action="store_true", help="only the packed-format fixture")
+    ap.add_argument("--meas-only", action="store_true", help="only the measurement fixtures")
     a = ap.parse_args()
     if a.build:
         subprocess.check_call([sys.executable, os.path.join(ROOT, "oracle", "build_ref.py"), "t4", "a6448"])
+    if a.meas_only:
+        for tag in ("t4", "a6448"):
+            make_meas(tag)
+        return
     if not a.packer_only:
         coeffs = coefficients()
         for tag in ("t4", "a6448"):
             make(tag, coeffs)
     make_packer("t4")
+    for tag in ("t4", "a6448"):
+        make_meas(tag)
 
 
 if __name__ == "__main__":
