@@ -306,6 +306,12 @@ def reference_msolve_timing(tag, u, b, shifts, np, iters, nrhs):
 
 NF_ML, NF_MS, NF_BETA, NF_DEG = 0.01, 0.05, 5.8, 15
 
+# DRAM bytes per output site of dslash_kernel<L64_18,1>, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum of its first timed launch at 24^4:
+# 200,237,056 + 6,219,008 bytes over Vh = 165,888 sites); the kernel streams per site, so the
+# traffic of a launch is this times Vh
+DSLASH_F64_18_DRAM_PER_SITE = (200237056 + 6219008) / 165888
+
 
 def _timed(torch, stream, fn, reps):
     """Average device time (ms) of fn() issued reps times on stream, CUDA events on that stream."""
@@ -894,7 +900,9 @@ def main():
                        "lattice": list(DIMS), "parallelism": "replicas%d" % world,
                        "l2": "inputs larger than L2 (links 604 MB)"},
             "roofline": {"bound": "hbm", "achieved": round(r["achieved"], 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(r["achieved"] / peak, 4), "traffic": None,
+                         "frac": round(r["achieved"] / peak, 4), "traffic": round(DSLASH_F64_18_DRAM_PER_SITE * Vh),
+                         "traffic_note": "ncu dram read+write of this kernel at 24^4 (1244.8 B per output site), "
+                                         "scaled to this launch by Vh",
                          "peak_kind": peak_kind, "kernel": "dslash_kernel<L64_18,1>",
                          "bytes_per_launch": half_dslash_bytes(0, Vh)},
             "gflops": round(r["gflops"], 1),
