@@ -310,13 +310,26 @@ int rhmc_dslash_host(rhmc_ctx *c, int parity_out, double *out, const double *in)
         return RHMC_OK;
     }
     if (!c->dh_ready) {
-        CK(cudaStreamCreateWithFlags(&c->dh_cmp, cudaStreamNonBlocking));
-        CK(cudaStreamCreateWithFlags(&c->dh_down, cudaStreamNonBlocking));
-        for (int i = 0; i < RHMC_DH_MAXCH; i++) {
-            CK(cudaEventCreateWithFlags(&c->dh_up_ev[i], cudaEventDisableTiming));
-            CK(cudaEventCreateWithFlags(&c->dh_cmp_ev[i], cudaEventDisableTiming));
+        // all or nothing: on a failure the handles made so far are released again
+        cudaStream_t st[2] = {nullptr, nullptr};
+        cudaEvent_t ev[2 * RHMC_DH_MAXCH + 1] = {};
+        cudaError_t e = cudaStreamCreateWithFlags(&st[0], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st[1], cudaStreamNonBlocking);
+        for (int i = 0; i < 2 * RHMC_DH_MAXCH + 1 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            for (cudaStream_t s : st)
+                if (s) cudaStreamDestroy(s);
+            for (cudaEvent_t v : ev)
+                if (v) cudaEventDestroy(v);
+            return cuda_fail(e, "rhmc_dslash_host streams");
         }
-        CK(cudaEventCreateWithFlags(&c->dh_done, cudaEventDisableTiming));
+        c->dh_cmp = st[0];
+        c->dh_down = st[1];
+        for (int i = 0; i < RHMC_DH_MAXCH; i++) {
+            c->dh_up_ev[i] = ev[i];
+            c->dh_cmp_ev[i] = ev[RHMC_DH_MAXCH + i];
+        }
+        c->dh_done = ev[2 * RHMC_DH_MAXCH];
         c->dh_ready = true;
     }
     // The library stream uploads chunk by chunk; the compute stream runs the Dslash of chunk j
