@@ -92,10 +92,11 @@ def test_mdagm_vs_oracle(oracle_mod):
         assert rel_err(got, ref) < 1e-13
 
 
-@pytest.mark.parametrize("dims", [(4, 4, 4, 4), (4, 6, 2, 10), (4, 4, 4, 2), (8, 8, 8, 16)])
+@pytest.mark.parametrize("dims", [(4, 4, 4, 4), (4, 6, 2, 10), (4, 4, 2, 14), (4, 4, 4, 2), (2, 4, 2, 34), (8, 8, 8, 16)])
 def test_dslash_host_reference_facing(oracle_mod, dims):
-    """Host arrays in the reference's layout: uploaded, applied and downloaded in chunks of
-    t-slabs (4, 5 and 8 chunks here; nt = 2 has too few slabs and runs unchunked)."""
+    """Host arrays in the reference's layout: uploaded, applied and downloaded in chunks of whole
+    t-slabs, the largest count in [3, 16] that divides nt (4, 10, 14 and 16 chunks here); nt = 2
+    and nt = 34 have no such count and run unchunked."""
     from gpu_util import new_ctx
     ctx = new_ctx(dims)
     u = F.random_links(dims, seed=21)
