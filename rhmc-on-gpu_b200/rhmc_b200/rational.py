@@ -60,9 +60,15 @@ def inverse_power(q, n, eps, optimise=True, grid=3000):
     return 0.0, a, b, err
 
 
-def rational_power(p, n, eps, optimise=True):
+def rational_power(p, n, eps, optimise=True, method="lsq"):
     """Coefficients of x^p on [eps, 1], p in (-1, 0) or (0, 1), degree n.
-    Returns dict(a0, a, b, min_eps, power, max_rel_err)."""
+    Returns dict(a0, a, b, min_eps, power, max_rel_err).  method "lsq": the pole-optimised least
+    squares fit above (a0 = 0 for negative powers); "minimax": minimax_power (type (n, n),
+    near-minimax relative error, usually orders of magnitude smaller at the same degree)."""
+    if method == "minimax":
+        return minimax_power(p, n, eps)
+    if method != "lsq":
+        raise ValueError("method must be 'lsq' or 'minimax'")
     if 0.0 < -p < 1.0:
         a0, a, b, err = inverse_power(-p, n, eps, optimise)
     elif 0.0 < p < 1.0:
@@ -85,3 +91,84 @@ def rescale(approx, lam_max, exponent):
     lam_max is the already enlarged bound (the reference multiplies findminmax's max by 1.05)."""
     e = lam_max ** exponent
     return {"a0": approx["a0"] * e, "a": [v * lam_max * e for v in approx["a"]], "b": [v * lam_max for v in approx["b"]]}
+
+
+def _aaa_lawson(x, f, m, lawson):
+    """Barycentric rational r(x) = sum_j w_j f_j/(x - z_j) / sum_j w_j/(x - z_j) of type
+    (m-1, m-1) minimising the relative error |r/f - 1| on the points x: AAA (Nakatsukasa, Sete and
+    Trefethen, SIAM J. Sci. Comput. 40 (2018) A1494) picks the support points z_j greedily, then
+    Lawson's iteratively reweighted least squares (Nakatsukasa and Trefethen, SIAM J. Sci. Comput.
+    42 (2020) A3157) moves the weights towards the minimax solution.  Returns (z, f_z, w, err)."""
+    rest = np.ones(len(x), bool)
+    r = np.full_like(f, np.mean(f))
+    z, fz = [], []
+    for _ in range(m):
+        e = np.where(rest, np.abs(r / f - 1.0), -1.0)
+        j = int(np.argmax(e))
+        z.append(x[j])
+        fz.append(f[j])
+        rest[j] = False
+        zz, ff = np.array(z), np.array(fz)
+        C = 1.0 / (x[rest][:, None] - zz[None, :])
+        A = (f[rest][:, None] - ff[None, :]) * C / f[rest][:, None]  # linearised relative error
+        w = np.linalg.svd(A, full_matrices=False)[2][-1]
+        r = f.copy()
+        r[rest] = (C @ (w * ff)) / (C @ w)
+    zz, ff = np.array(z), np.array(fz)
+    C = 1.0 / (x[rest][:, None] - zz[None, :])
+    A = (f[rest][:, None] - ff[None, :]) * C / f[rest][:, None]
+    wt = np.full(A.shape[0], 1.0 / A.shape[0])
+    best = (np.inf, None)
+    for _ in range(lawson):
+        w = np.linalg.svd(np.sqrt(wt)[:, None] * A, full_matrices=False)[2][-1]
+        e = np.abs((C @ (w * ff)) / (C @ w) / f[rest] - 1.0)
+        if e.max() < best[0]:
+            best = (e.max(), w.copy())
+        wt = wt * e
+        wt /= wt.sum()
+    return zz, ff, best[1], best[0]
+
+
+def _bary_poles(z, w):
+    """Poles of a barycentric rational: the finite eigenvalues of the pencil
+    ([0 w^T; 1 diag(z)], diag(0, 1, ..., 1))."""
+    from scipy.linalg import eig
+    m = len(z)
+    E = np.zeros((m + 1, m + 1))
+    E[0, 1:] = w
+    E[1:, 0] = 1.0
+    E[1:, 1:] = np.diag(z)
+    B = np.eye(m + 1)
+    B[0, 0] = 0.0
+    ev = eig(E, B, right=False)
+    return ev[np.isfinite(ev)]
+
+
+def minimax_power(p, n, eps, grid=4000, lawson=150):
+    """x^p on [eps, 1], p in (-1, 0) or (0, 1), as a0 + sum_i a_i/(x + b_i) with n poles: a
+    near-minimax approximation of type (n, n) in the relative error (the kind the reference's
+    AlgRemez produces, rationalapprox_calc.cc:8-177), from AAA-Lawson.  The poles are the
+    barycentric form's (all real and negative for these powers; anything else raises
+    ValueError); the numerators are then taken from the barycentric form or from a least-squares
+    fit of the relative error, whichever has the smaller maximum error on a 4x finer grid.
+    Returns the dictionary of rational_power."""
+    if not (0.0 < abs(p) < 1.0):
+        raise ValueError("power must be in (-1, 0) or (0, 1)")
+    x = np.geomspace(eps, 1.0, grid)
+    f = x ** p
+    z, fz, w, _ = _aaa_lawson(x, f, n + 1, lawson)
+    pol = _bary_poles(z, w)
+    if len(pol) != n or np.any(np.abs(pol.imag) > 1e-9 * np.abs(pol)) or np.any(pol.real >= 0.0):
+        raise ValueError("the approximation of x^%g with %d poles has poles off the negative real axis" % (p, n))
+    b = np.sort(-pol.real)
+    xf = np.geomspace(eps, 1.0, 4 * grid)
+    ffine = xf ** p
+    # numerators from the barycentric form: a0 = r(inf), a_i = N(-b_i) / D'(-b_i)
+    N = lambda t: np.sum(w * fz / (t - z))
+    dD = lambda t: -np.sum(w / (t - z) ** 2)
+    cand = [np.concatenate([[np.sum(w * fz) / np.sum(w)], [N(-bi) / dD(-bi) for bi in b]]),
+            _fit(xf, ffine, b, True)]
+    errs = [np.max(np.abs(_eval(xf, b, c, True) / ffine - 1.0)) for c in cand]
+    c = cand[int(np.argmin(errs))]
+    return {"a0": float(c[0]), "a": [float(v) for v in c[1:]], "b": [float(v) for v in b], "min_eps": float(eps),
+            "power": float(p), "max_rel_err": float(min(errs)), "method": "aaa-lawson"}

@@ -21,11 +21,14 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def _setup(two_species=False):
+def _setup(two_species=False, minimax=False):
     from gpu_util import new_ctx
     g = dict(np.load(os.path.join(HERE, "golden", "ref_t4.npz")))
     with open(os.path.join(HERE, "golden", "rational_coeffs.json")) as f:
         cf = json.load(f)["t4"]
+    if minimax:  # near-minimax type (n, n) coefficients: a0 != 0 in the action's approximation
+        from rhmc_b200 import rational as R
+        cf = [R.rational_power(c["power"], len(c["a"]), c["min_eps"], method="minimax") for c in cf]
     m = float(g["mass"])
     ctx = new_ctx(tuple(g["dims"]), mass=m, beta=float(g["beta"]))
     ctx.driver_setup(no_flavours=2, no_ps=1, residue_md=1e-13, residue_metro=1e-13)
@@ -54,9 +57,9 @@ def _fd(ctx, u, l, Q, action, h, four_point):
     return (S(h) - S(-h)) / (2 * h)
 
 
-@pytest.mark.parametrize("part", ["fermion", "fermion_2species", "gauge"])
+@pytest.mark.parametrize("part", ["fermion", "fermion_2species", "fermion_minimax", "gauge"])
 def test_force_is_the_derivative_of_its_action(part):
-    ctx, g = _setup(part == "fermion_2species")
+    ctx, g = _setup(part == "fermion_2species", part == "fermion_minimax")
     u = g["u"]
     rng = np.random.Generator(np.random.Philox(6006))
     links = rng.choice(u.shape[0], size=4, replace=False)
