@@ -1,5 +1,5 @@
 // msolve.cu -- host orchestration of the multi-shift CG (msolve.cuh): workspace, CUDA-graph
-// capture of a chunk of iterations, device-flag polling, and the extern "C" entry points.
+// capture of one delayed-update window of iterations, device-flag polling, and the extern "C" entry points.
 #include <cmath>
 #include <cstring>
 #include <vector>

@@ -14,13 +14,15 @@
 // solver's criterion, cuda_inverter.cu:777-785) or at max_iter.  sigma_0 is the base shift
 // (0 in the reference; the mixed solver uses the smallest pole) and sigma_i are relative to it.
 //
-// Kernel sequence per iteration (one CUDA graph replays a chunk of iterations):
+// Kernel sequence per iteration (one CUDA graph replays a window of MS_WIN iterations):
 //   K1 D_oe:    h = D_oe p                                   (Dslash, NR right-hand sides)
 //   K2 D_eo:    s = (m^2+sigma_0) p - D_eo h, Re<p,s>        (Dslash epilogue + FP64 reduction;
 //               the last block computes omega, zeta''', omega_i for every RHS)
-//   K3 resid:   r += omega s, |r|^2                          (last block: gamma, gamma_i, freezing,
+//   K3 resid:   r += omega s, |r|^2 into the window's ring   (last block: gamma, gamma_i, freezing,
 //               convergence, stop flag)
-//   K4 update:  p = r + gamma p; x_i -= omega_i p_i; p_i = zeta''' r + gamma_i p_i
+//   K4 update:  p = r + gamma p
+// and once per window the flush kernel applies the window's x_i -= omega_i p_i and
+// p_i = zeta''' r + gamma_i p_i of every shift, composed from the recorded scalars and residuals.
 // Scalars live in device memory (MSState) and never leave the GPU during the solve; the host
 // only polls the stop flag between graph replays.
 #pragma once

@@ -14,7 +14,7 @@ struct MSolveArgs {
     double res_base;      // stop when sqrt(|r|^2) <= res_base
     int max_iter;
     int stop_on_frozen;
-    int chunk;            // iterations per captured graph
+    int chunk;            // iterations per captured graph (the multi-shift loop uses its window, MS_WIN)
     const void *b;        // FP64 internal spinors, nrhs of them
     void *x;              // internal spinors of the link format's precision, [nrhs][nshift]
 };
