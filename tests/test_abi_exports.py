@@ -44,3 +44,21 @@ def test_errors_without_a_context():
     assert lib.rhmc_create(None, None) == -1  # RHMC_ERR_ARG
     assert b"null" in lib.rhmc_last_error()
     assert lib.rhmc_destroy(None) == 0
+
+
+def test_headers_are_plain_c(tmp_path):
+    """Both headers compile as pedantic C99 and a C program links against the library (the
+    boundary needs no C++); destroying a null context is a no-op that returns RHMC_OK."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "abi.c"
+    src.write_text('#include "rhmc_b200.h"\n#include "rhmc_legacy.h"\n'
+                   "int main(void) { rhmc_params p = {4, 4, 4, 4, 0, 0.1, 5.5, 0}; (void)p;\n"
+                   "  return rhmc_destroy((rhmc_ctx *)0); }\n")
+    libdir = os.path.join(ROOT, "rhmc-on-gpu_b200")  # the in-tree build
+    exe = tmp_path / "abi"
+    subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I" + os.path.join(ROOT, "include"),
+                           str(src), "-L" + libdir, "-lrhmc_b200", "-Wl,-rpath," + libdir, "-o", str(exe)])
+    assert subprocess.run([str(exe)]).returncode == 0
