@@ -1,14 +1,17 @@
 // noalloc.cu -- FP64 true residuals |b_r - (M^dag M + sigma_i) x_{r,i}| that allocate no device
 // memory (rhmc_true_residuals_noalloc).
 //
-// Who needs it: a caller that checks its solutions at a point where it cannot call cudaMalloc.
-// Typical cases are code that is recording its GPU work into a CUDA graph (an allocation made
-// during stream capture is not part of the graph and cudaMalloc may synchronise the whole
-// device), and host programs that hand all device memory to their own pool at start-up and
-// forbid allocation afterwards.  rhmc_true_residuals takes its two intermediate spinors and
-// its reduction partials from the context's grow-on-demand workspace, which calls cudaMalloc
-// the first time (and whenever a larger size is needed); this variant takes them from one
-// fixed array instead.
+// Who needs it: a caller that checks its solutions at a point where it must not call
+// cudaMalloc.  Host programs that hand all device memory to their own pool at start-up treat
+// any later allocation as an error; long Markov chains that share a GPU under a fixed memory
+// budget cannot risk an out-of-memory failure hours into a run; and code that keeps work in
+// flight on other streams cannot accept the device-wide synchronisation cudaMalloc may
+// imply.  rhmc_true_residuals takes its two intermediate spinors and its reduction partials
+// from the context's grow-on-demand workspace, which calls cudaMalloc the first time (and
+// whenever a larger size is needed); this variant takes them from one fixed array instead.
+//
+// The call is host-synchronous: it waits for the context's stream and copies the residuals
+// into the caller's host array before it returns.
 //
 // Scratch: the file-scope device array g_noalloc_scratch below, RHMC_NOALLOC_SCRATCH_BYTES
 // (about 6.3 MB), which every GPU that loads the library holds until the process exits.
@@ -23,7 +26,8 @@
 //
 // Device address: host code cannot use the array's name as a device pointer (it names a host
 // shadow).  The first call on a device, with that device current, looks the address up with
-// cudaGetSymbolAddress and caches it; make that first call before any stream capture.
+// cudaGetSymbolAddress and caches it (this set-up is part of that first call); make that first
+// call before any stream capture.
 #include <cmath>
 #include <mutex>
 

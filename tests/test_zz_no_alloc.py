@@ -1,9 +1,10 @@
-"""rhmc_true_residuals_noalloc: the FP64 true-residual check for callers that cannot allocate
-device memory at that point (recording a CUDA graph, an application-owned memory pool).  It
-must give the values of rhmc_true_residuals, which takes its scratch from the context's
-workspace, call after call although its fixed scratch array keeps the previous call's
-contents, and refuse sizes beyond its fixed limit.  Collected last on purpose: if it fails,
-a run that stops at the first failure has already run every other test."""
+"""rhmc_true_residuals_noalloc: the FP64 true-residual check for callers that must not allocate
+device memory at that point (a program whose own pool owns all device memory, a chain sharing
+the GPU under a fixed memory budget).  It must give the values of rhmc_true_residuals, which
+takes its scratch from the context's workspace, call after call although its fixed scratch
+array keeps the previous call's contents; it must leave the device's free memory unchanged;
+and it must refuse sizes beyond its fixed limit.  Collected last on purpose: if it fails, a
+run that stops at the first failure has already run every other test."""
 import ctypes
 
 import numpy as np
@@ -44,6 +45,35 @@ def test_noalloc_matches_workspace_version_on_consecutive_calls():
         rc, out = _noalloc(ctx, x, b, shifts, nrhs)
         assert rc == 0, rb.lib().rhmc_last_error()
         np.testing.assert_allclose(out, ref, rtol=1e-12, atol=0)
+
+
+def test_noalloc_leaves_free_device_memory_unchanged():
+    """On a fresh context whose workspace has never been used by a true-residual check, repeated
+    calls do not change the device's free memory, while the workspace version does grow it."""
+    import torch
+    from gpu_util import new_ctx, to_internal
+    dims = (8, 8, 8, 16)
+    ctx = new_ctx(dims, mass=0.05)
+    ctx.set_gauge(F.random_links(dims, seed=911))
+    shifts = np.array([0.0, 0.2])
+    b = to_internal(ctx, rb.LINKS_F64_18, F.random_spinor(dims, seed=912))
+    x = to_internal(ctx, rb.LINKS_F64_18, F.random_spinor(dims, seed=913, n=len(shifts)))
+    torch.cuda.synchronize()
+    # the first call may load the library's kernels onto the device (module loading is lazy)
+    rc, first = _noalloc(ctx, x, b, shifts, 1)
+    assert rc == 0, rb.lib().rhmc_last_error()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        rc, out = _noalloc(ctx, x, b, shifts, 1)
+        assert rc == 0, rb.lib().rhmc_last_error()
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+        np.testing.assert_array_equal(out, first)
+    ref = ctx.true_residuals(x, b, shifts, 1)  # grow-on-demand workspace: allocates
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] < free0
+    np.testing.assert_allclose(first, ref, rtol=1e-12, atol=0)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
