@@ -255,6 +255,8 @@ def msolve_bench(rb, F, np, torch, rank, dev, stream, dims=None, relative=False,
                      "refine_iters": sum(i["refine_iters"] for i in infos),
                      "s_phase_a": round(sum(i["seconds_phase_a"] for i in infos), 4),
                      "systems_refined": sum(i["systems_refined"] for i in infos),
+                     "iters_fp64": sum(i["iters_fp64"] for i in infos) if batched else None,
+                     "ms_reliable_updates": sum(i["ms_reliable_updates"] for i in infos),
                      "links": rb.FMT_NAMES[fmt]}
     mixed = [k for k in ("mixed_batched", "mixed_batched_f32_bulk", "mixed_batched_f32_bulk_f16_refine") if k in out]
     if "fp64_single_rhs" in out and mixed:

@@ -121,11 +121,14 @@ enum {
     RHMC_MSOLVE_FP64 = 0,  /* the reference algorithm in FP64 (multips_shifted_invert,
                               lib/Action/Inverter/inverter.cc:142-339): base operator M^dag M,
                               shift frozen when sqrt(|r|^2 zeta^2) < residual */
-    RHMC_MSOLVE_MIXED = 1, /* multi-shift on the smallest pole with all RHS batched (FP32 links and
-                              vectors to tol_phase_a |b| with an FP32 fmt; FP64 vectors to
-                              `residual` with an FP64 fmt, 12-real links when fmt says so), then
-                              FP32 CG per system inside FP64 defect correction until every FP64
-                              true residual |b - (M^dag M + sigma_i) x_i| <= residual */
+    RHMC_MSOLVE_MIXED = 1, /* multi-shift on the smallest pole with all RHS batched.  FP32 or half
+                              fmt: precision schedule -- FP64 vectors and 12-real FP64 links until
+                              |r| <= tol_phase_a |b|, then the same recurrences resumed with FP32
+                              links and base vectors (FP64 shifted vectors, FP64 reliable update of
+                              the base residual every 32 iterations) to `residual`.  FP64 fmt: FP64
+                              vectors throughout (12-real links when fmt says so).  Then FP32 CG
+                              per system inside FP64 defect correction for every system whose FP64
+                              true residual |b - (M^dag M + sigma_i) x_i| is still above `residual` */
     RHMC_MSOLVE_FP32 = 2   /* the reference algorithm with FP32 links and vectors (its
                               single-precision path, lib/Cuda/cuda_inverter.cu:647-857, used
                               when residual >= 1e-4, cu_inverter.cc:45-60); FP64 scalars */
@@ -142,7 +145,8 @@ typedef struct {
                               FP32 ones for RHMC_MSOLVE_FP32, any for RHMC_MSOLVE_MIXED; in mixed mode
                               RHMC_LINKS_F16_12 means an FP32 12-real multi-shift phase followed by a
                               refinement whose sloppy CG runs on half links and half spinors) */
-    double tol_phase_a;    /* mixed mode: relative residual of the FP32 multi-shift phase (0: 3e-6) */
+    double tol_phase_a;    /* mixed mode, FP32/half fmt: relative residual |r|/|b| at which the FP64
+                              part of the precision schedule hands over to FP32 (0: 1e-3) */
     double ru_delta;       /* mixed mode: FP32 residual reduction between FP64 updates (0: 0.05) */
     int certify;           /* FP64 mode: afterwards refine, by FP64 CG one system at a time, every system
                               whose FP64 true residual is still above `residual` (the reference's
@@ -154,12 +158,17 @@ typedef struct {
 
 typedef struct {
     int status;            /* RHMC_OK or the error returned */
-    int iters[8];          /* multi-shift iterations per RHS (first 8) */
+    int iters[8];          /* multi-shift iterations of right-hand sides 0..7 only (see iters_total
+                              and iters_max for any nrhs) */
     long refine_iters;     /* mixed mode: batched refinement iterations (sum over batches) */
     int reliable_updates;  /* mixed mode: FP64 residual recomputations */
     double seconds;        /* wall time of the call */
     double seconds_phase_a;/* mixed mode / certified FP64: wall time of the multi-shift phase */
     int systems_refined;   /* mixed mode / certified FP64: (rhs, shift) systems that needed refinement */
+    long iters_total;      /* multi-shift iterations summed over every right-hand side */
+    int iters_max;         /* largest multi-shift iteration count of any right-hand side */
+    long iters_fp64;       /* mixed mode: multi-shift iterations run in FP64 (summed over RHS 0..7) */
+    int ms_reliable_updates; /* mixed mode, FP32/half fmt: FP64 reliable updates of the multi-shift */
 } rhmc_msolve_info;
 
 /* (M^dag M + sigma_i) x_{r,i} = b_r for every shift i and RHS r (cuda_shifted_inverter /
@@ -312,14 +321,18 @@ int rhmc_driver_stats(rhmc_ctx *ctx, long *force_evals, long *solves);
 int rhmc_fma_peak(rhmc_ctx *ctx, int fp64, double *tflops);
 
 /* No counterpart in the reference.  The same values as rhmc_true_residuals, for callers that
- * cannot allocate device memory where they check their solutions (for example while recording
- * into a CUDA graph, or under an application-owned memory pool): this entry point takes its
- * scratch from one fixed device array compiled into the library (RHMC_NOALLOC_SCRATCH_BYTES,
- * held on every GPU that loads the library until the process exits) and calls no allocator.
- * Limits: Vh <= RHMC_NOALLOC_MAX_VH sites per parity and nrhs*nshift <= RHMC_NOALLOC_MAX_SYSTEMS;
- * larger requests return RHMC_ERR_ARG.  The array is shared by all calls on a device: calls whose
- * GPU work overlaps race.  The first call on a device looks up the array's device address; make
- * it before any stream capture.  x, b: FP64 internal device spinors; out: host double[nrhs][nshift]. */
+ * must not allocate device memory where they check their solutions: programs whose own pool
+ * owns all device memory after start-up, chains sharing a GPU under a fixed memory budget, and
+ * code that cannot accept the device-wide synchronisation an allocation may imply.  This entry
+ * point takes its scratch from one fixed device array compiled into the library
+ * (RHMC_NOALLOC_SCRATCH_BYTES, held on every GPU that loads the library until the process
+ * exits) and calls no allocator.  Limits: Vh <= RHMC_NOALLOC_MAX_VH sites per parity and
+ * nrhs*nshift <= RHMC_NOALLOC_MAX_SYSTEMS; larger requests return RHMC_ERR_ARG.  The array is
+ * shared by all calls on a device and keeps the last call's contents: calls whose GPU work
+ * overlaps race.  The call is host-synchronous (it waits for the context's stream and writes
+ * `out` before returning).  The first call on a device looks up the array's device address
+ * with that device current; make it before any stream capture.  x, b: FP64 internal device
+ * spinors; out: host double[nrhs][nshift]. */
 #define RHMC_NOALLOC_MAX_VH 65536
 #define RHMC_NOALLOC_MAX_SYSTEMS 256
 #define RHMC_NOALLOC_SCRATCH_BYTES (2u * 3u * 65536u * 16u + 256u * 8u + 256u * 8u)

@@ -11,12 +11,13 @@ bool fmt_is_f64(int fmt) { return fmt == RHMC_LINKS_F64_18 || fmt == RHMC_LINKS_
 int dslash_grid(rhmc_ctx *c) { return grid_for(c->Vh, DSLASH_MIN_BLOCK); }
 
 template <class LF, int NR>
-static void run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in, size_t stride, const void *y,
-                double alpha, double beta, double *partials)
+static cudaError_t run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in, size_t stride, const void *y,
+                       double alpha, double beta)
 {
     typedef typename LF::real R;
     typedef typename LF::store::elem E;
     DslashArgs<LF, NR> a;
+    memset(&a, 0, sizeof(a));
     a.g = c->g;
     a.p_out = p_out;
     a.links = lf;
@@ -26,42 +27,34 @@ static void run(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in,
     a.stride = stride;
     a.alpha = (R)alpha;
     a.beta = (R)beta;
-    a.use_alphas = 0;
     for (int r = 0; r < NR; r++) a.alphas[r] = (R)alpha;
-    a.partials = partials;
-    a.ticket = nullptr;
-    a.stop = nullptr;
-    a.stop_set = nullptr;
-    a.run_if = nullptr;
-    a.k_lo = 0;
-    a.k_count = 0;
-    constexpr int B = DslashCfg<LF, NR, false>::block;
-    const int grid = grid_for(c->Vh, B);
-    if (y) dslash_kernel<LF, NR, true, false, NoFin><<<grid, B, 0, c->stream>>>(a);
-    else dslash_kernel<LF, NR, false, false, NoFin><<<grid, B, 0, c->stream>>>(a);
     c->launches++;
+    if (y) return dslash_launch<LF, NR, true, false, NoFin>(a, (int)c->Vh, c->stream);
+    return dslash_launch<LF, NR, false, false, NoFin>(a, (int)c->Vh, c->stream);
 }
 
 template <class LF>
-static void run_n(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in, size_t stride, int n, const void *y,
-                  double alpha, double beta, double *partials)
+static cudaError_t run_n(rhmc_ctx *c, const LF &lf, int p_out, void *out, const void *in, size_t stride, int n, const void *y,
+                         double alpha, double beta)
 {
     switch (n) {
-    case 1: run<LF, 1>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
-    case 2: run<LF, 2>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
-    case 3: run<LF, 3>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
-    case 4: run<LF, 4>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
-    case 8: run<LF, 8>(c, lf, p_out, out, in, stride, y, alpha, beta, partials); break;
+    case 1: return run<LF, 1>(c, lf, p_out, out, in, stride, y, alpha, beta);
+    case 2: return run<LF, 2>(c, lf, p_out, out, in, stride, y, alpha, beta);
+    case 3: return run<LF, 3>(c, lf, p_out, out, in, stride, y, alpha, beta);
+    case 4: return run<LF, 4>(c, lf, p_out, out, in, stride, y, alpha, beta);
+    case 8: return run<LF, 8>(c, lf, p_out, out, in, stride, y, alpha, beta);
     default: {
         // split into supported widths
         typedef typename LF::store::elem E;
         int done = 0;
         while (done < n) {
             int m = n - done >= 8 ? 8 : (n - done >= 4 ? 4 : n - done);
-            run_n<LF>(c, lf, p_out, (E *)out + done * stride, (const E *)in + done * stride, stride, m,
-                      y ? (const E *)y + done * stride : nullptr, alpha, beta, nullptr);
+            const cudaError_t e = run_n<LF>(c, lf, p_out, (E *)out + done * stride, (const E *)in + done * stride, stride, m,
+                                            y ? (const E *)y + done * stride : nullptr, alpha, beta);
+            if (e != cudaSuccess) return e;
             done += m;
         }
+        return cudaSuccess;
     }
     }
 }
@@ -88,10 +81,8 @@ cudaError_t launch_dslash_f64_range(rhmc_ctx *c, cudaStream_t s, int p_out, void
     a.beta = 0.5;
     a.k_lo = k_lo;
     a.k_count = k_count;
-    constexpr int B = DslashCfg<L64_18, 1, false>::block;
-    dslash_kernel<L64_18A, 1, false, false, NoFin><<<grid_for(k_count, B), B, 0, s>>>(a);
     c->launches++;
-    return cudaGetLastError();
+    return dslash_launch<L64_18A, 1, false, false, NoFin>(a, k_count, s);
 }
 
 cudaError_t launch_dslash(rhmc_ctx *c, int fmt, int p_out, void *out, const void *in, size_t stride, int n,
@@ -101,15 +92,14 @@ cudaError_t launch_dslash(rhmc_ctx *c, int fmt, int p_out, void *out, const void
     if (nblocks) *nblocks = dslash_grid(c);
     cudaError_t e = cudaSuccess;
     switch (fmt) {
-    case RHMC_LINKS_F64_18: { L64_18 lf; e = links_f64_18(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
-    case RHMC_LINKS_F64_12: { L64_12 lf; e = links_f64_12(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
-    case RHMC_LINKS_F32_18: { L32_18 lf; e = links_f32_18(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
-    case RHMC_LINKS_F32_12: { L32_12 lf; e = links_f32_12(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
-    case RHMC_LINKS_F16_12: { L16_12 lf; e = links_f16_12(c, &lf); if (!e) run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta, partials); break; }
+    case RHMC_LINKS_F64_18: { L64_18 lf; e = links_f64_18(c, &lf); if (!e) e = run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta); break; }
+    case RHMC_LINKS_F64_12: { L64_12 lf; e = links_f64_12(c, &lf); if (!e) e = run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta); break; }
+    case RHMC_LINKS_F32_18: { L32_18 lf; e = links_f32_18(c, &lf); if (!e) e = run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta); break; }
+    case RHMC_LINKS_F32_12: { L32_12 lf; e = links_f32_12(c, &lf); if (!e) e = run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta); break; }
+    case RHMC_LINKS_F16_12: { L16_12 lf; e = links_f16_12(c, &lf); if (!e) e = run_n(c, lf, p_out, out, in, stride, n, y, alpha, beta); break; }
     default: return cudaErrorInvalidValue;
     }
-    if (e != cudaSuccess) return e;
-    return cudaGetLastError();
+    return e;
 }
 
 }  // namespace rhmc

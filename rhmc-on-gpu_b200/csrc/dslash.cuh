@@ -71,27 +71,29 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
     const int k = a.k_lo + blockIdx.x * blockDim.x + threadIdx.x;
     const int Vh = a.g.Vh;
     const int kend = a.k_count ? a.k_lo + a.k_count : Vh;
-    // y (read only by the epilogue) is fetched into shared memory by cp.async at the start, so its
-    // DRAM latency overlaps the stencil instead of following it (when the block's copy fits)
     typedef typename LF::store S;
     typedef typename S::elem E;
+    // y (read only by the epilogue) is fetched into shared memory by cp.async at the start, so its
+    // DRAM latency overlaps the stencil instead of following it (when the block's copy fits)
     constexpr bool PF = HAS_Y && S::soa && (NR * S::planes * BLOCK * sizeof(E) <= 24576);
     __shared__ __align__(16) E ysm[PF ? NR * S::planes * BLOCK : 1];
-    if (PF && k < kend) {
+    Site s = site_of(a.g, a.p_out, k < kend ? k : a.k_lo);
+    if (k < kend) {
+        if (PF) {
 #pragma unroll
-        for (int r = 0; r < NR; r++)
+            for (int r = 0; r < NR; r++)
 #pragma unroll
-            for (int pl = 0; pl < S::planes; pl++)
-                cp_async_elem<sizeof(E)>(&ysm[(r * S::planes + pl) * BLOCK + threadIdx.x],
-                                         a.y + r * a.stride + (size_t)pl * Vh + k);
-        cp_async_commit();
+                for (int pl = 0; pl < S::planes; pl++)
+                    cp_async_elem<sizeof(E)>(&ysm[(r * S::planes + pl) * BLOCK + threadIdx.x],
+                                             a.y + r * a.stride + (size_t)pl * Vh + k);
+            cp_async_commit();
+        }
     }
     double red[NR];
 #pragma unroll
     for (int j = 0; j < NR; j++) red[j] = 0.0;
 
     if (k < kend) {
-        const Site s = site_of(a.g, a.p_out, k);
         vec3<R> acc[NR];
 #pragma unroll
         for (int r = 0; r < NR; r++)
@@ -140,6 +142,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
         }
     }
     if (RED) reduce_finalize<NR>(red, a.partials, a.ticket, a.fin);
+}
+
+// One launch over `nsites` output sites (from a.k_lo) on stream s.
+template <class LF, int NR, bool HAS_Y, bool RED, class FIN, int BLOCK = DslashCfg<LF, NR, RED>::block,
+          int MINB = DslashCfg<LF, NR, RED>::minb>
+inline cudaError_t dslash_launch(const DslashArgs<LF, NR, FIN> &a, int nsites, cudaStream_t s)
+{
+    dslash_kernel<LF, NR, HAS_Y, RED, FIN, BLOCK, MINB><<<(nsites + BLOCK - 1) / BLOCK, BLOCK, 0, s>>>(a);
+    return cudaGetLastError();
 }
 
 }  // namespace rhmc

@@ -37,9 +37,14 @@ constexpr int VEC_BLOCK = 256;
 
 struct MSRhs {
     double delta, omega, omega_prev, gamma, lambda, alpha, b2;
+    double res;        // this phase stops the RHS when sqrt(lambda) <= res
     int iter;          // iterations performed
     int running;       // this iteration updates the RHS
     int running_next;  // still running after this iteration
+    int rslot;         // ring slot holding the current residual
+    int i0;            // index of the base shift (relative shift 0) among this RHS's poles
+    double ru_best;    // smallest true |r|^2 seen at a reliable update
+    int ru_stall;      // reliable updates since ru_best last fell by 4x
     double zeta_i[MS_MAX_SHIFT], zeta_ii[MS_MAX_SHIFT], zeta_iii[MS_MAX_SHIFT];
     double omegas[MS_MAX_SHIFT], gammas[MS_MAX_SHIFT];
     int active[MS_MAX_SHIFT];       // shift updated in this iteration
@@ -59,7 +64,12 @@ struct MSState {
     int nshift, nrhs, max_iter;
     int stop_on_frozen;             // also stop when every shift is frozen
     double res;                     // base residual target: stop when sqrt(lambda) <= res
+    double tau;                     // > 0: this phase stops an RHS once sqrt(lambda) <= tau |b| (a
+                                    // later phase in lower precision resumes it)
     double tgt[MS_MAX_SHIFT];       // freezing threshold for sqrt(delta zeta''^2)
+    // reliable updates (resumed lower-precision phase): every ru_every windows the base residual
+    // is recomputed in FP64 from the FP64 base solution and the base direction re-synchronised
+    int ru_every, ru_windows, ru_now, ru_count;
     MSRhs rhs[MS_MAX_RHS];
 };
 
@@ -79,6 +89,8 @@ struct FinInit {
             q.lambda = tot[r];
             q.alpha = 0.0;
             q.iter = 0;
+            q.rslot = MS_WIN - 1;
+            q.res = st->tau > 0.0 ? fmax(st->res, st->tau * sqrt(tot[r])) : st->res;
             q.running = 1;
             q.running_next = (tot[r] > 0.0) ? 1 : 0;  // b == 0: x = 0 is exact
             if (!isfinite(tot[r])) {
@@ -158,6 +170,7 @@ struct FinLambda {
                 MSRhs &q = st->rhs[r];
                 if (!q.running) continue;
                 q.lambda = tot[r];
+                q.rslot = st->wpos;
                 if (!isfinite(q.lambda)) {
                     st->status = 2;
                     q.running_next = 0;
@@ -190,7 +203,7 @@ struct FinLambda {
             for (int i = 0; i < ns; i++) nact += q.active[i] ? q.active_next[i] : 0;
             q.delta = q.lambda;
             q.iter++;
-            int done = (sqrt(q.lambda) <= st->res) || (st->stop_on_frozen && nact == 0);
+            int done = (sqrt(q.lambda) <= q.res) || (st->stop_on_frozen && nact == 0);
             if (!done && q.iter >= st->max_iter) {
                 done = 1;
                 st->status = (st->status == 0) ? 1 : st->status;
@@ -220,15 +233,17 @@ struct MSVec {
 };
 
 // x_i = 0, r_0 = p = p_i = b (b FP64 internal), |b|^2.  r_0 goes to the last slot of the
-// residual ring (the slot the first iteration reads).
-template <typename Rv, int NR>
+// residual ring (the slot the first iteration reads).  Base vectors (ring, p) are stored in Rv,
+// the shifted solutions and directions (x, ps) in Rx.
+template <typename Rv, typename Rx, int NR>
 __global__ void __launch_bounds__(VEC_BLOCK) ms_init_kernel(int Vh, int nshift, size_t stride, const double2 *__restrict__ b,
                                                              typename MSVec<Rv>::E *ring, typename MSVec<Rv>::E *p,
-                                                             typename MSVec<Rv>::E *ps, typename MSVec<Rv>::E *x,
+                                                             typename MSVec<Rx>::E *ps, typename MSVec<Rx>::E *x,
                                                              double *partials, unsigned *ticket, MSState *st)
 {
     typename MSVec<Rv>::E *r = ring + (size_t)(MS_WIN - 1) * NR * stride;
     typedef typename MSVec<Rv>::E E;
+    typedef typename MSVec<Rx>::E EX;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double red[NR];
 #pragma unroll
@@ -246,12 +261,14 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_init_kernel(int Vh, int nshift, 
                 e.y = (Rv)v.y;
                 r[o] = e;
                 p[o] = e;
-                E z;
+                EX ex, z;
+                ex.x = (Rx)v.x;
+                ex.y = (Rx)v.y;
                 z.x = 0;
                 z.y = 0;
                 for (int i = 0; i < nshift; i++) {
                     const size_t oi = (size_t)(j * nshift + i) * stride + (size_t)c * Vh + k;
-                    ps[oi] = e;
+                    ps[oi] = ex;
                     x[oi] = z;
                 }
             }
@@ -332,13 +349,13 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_update_kernel(int Vh, size_t str
 // block derive (cx0, cx, ca, cb) of one (rhs, shift) from the recorded scalars into shared memory
 // (skipping iterations where the shift was frozen), then every site applies them: each shifted
 // vector is read and written once per window instead of once per iteration.
-template <typename Rv, int NR>
+template <typename Rv, typename Rx, int NR>
 __global__ void __launch_bounds__(VEC_BLOCK) ms_flush_kernel(int Vh, int nshift, size_t stride,
                                                               const typename MSVec<Rv>::E *__restrict__ ring,
-                                                              typename MSVec<Rv>::E *ps, typename MSVec<Rv>::E *x,
+                                                              typename MSVec<Rx>::E *ps, typename MSVec<Rx>::E *x,
                                                               double *partials, unsigned *ticket, MSState *st)
 {
-    typedef typename MSVec<Rv>::E E;
+    typedef typename MSVec<Rx>::E E;
     __shared__ double s_cx0[NR * MS_MAX_SHIFT], s_ca[NR * MS_MAX_SHIFT];
     __shared__ double s_cx[NR * MS_MAX_SHIFT][MS_WIN], s_cb[NR * MS_MAX_SHIFT][MS_WIN];
     __shared__ int s_use[NR * MS_MAX_SHIFT];  // 0: nothing to do, 1: x only, 2: x and p
@@ -365,7 +382,9 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_flush_kernel(int Vh, int nshift,
             s_cx[t][m] = cx[m];
             s_cb[t][m] = cb[m];
         }
-        s_use[t] = any ? ((q.running_next && q.active_next[i]) ? 2 : 1) : 0;
+        // p_i is written for every shift still active, also when the RHS stopped in this window:
+        // a later phase may resume it from exactly this state
+        s_use[t] = any ? (q.active_next[i] ? 2 : 1) : 0;
     }
     __syncthreads();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -377,12 +396,16 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_flush_kernel(int Vh, int nshift,
                 E rv[MS_WIN];
 #pragma unroll
                 for (int m = 0; m < MS_WIN; m++)
-                    if (m < wp) rv[m] = ring[((size_t)m * NR + j) * stride + (size_t)c * Vh + k];
+                    if (m < wp) {
+                        const typename MSVec<Rv>::E q = ring[((size_t)m * NR + j) * stride + (size_t)c * Vh + k];
+                        rv[m].x = (Rx)q.x;
+                        rv[m].y = (Rx)q.y;
+                    }
                 for (int i = 0; i < nshift; i++) {
                     const int t = j * nshift + i, use = s_use[t];
                     if (!use) continue;
                     const size_t o = (size_t)t * stride + (size_t)c * Vh + k;
-                    const Rv x0 = (Rv)s_cx0[t], a0 = (Rv)s_ca[t];
+                    const Rx x0 = (Rx)s_cx0[t], a0 = (Rx)s_ca[t];
                     const E p0 = ps[o];
                     E xv = x[o];
                     E pv;
@@ -393,7 +416,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_flush_kernel(int Vh, int nshift,
 #pragma unroll
                     for (int m = 0; m < MS_WIN; m++) {
                         if (m >= wp) break;
-                        const Rv cx = (Rv)s_cx[t][m], cb = (Rv)s_cb[t][m];
+                        const Rx cx = (Rx)s_cx[t][m], cb = (Rx)s_cb[t][m];
                         xv.x = xv.x - cx * rv[m].x;
                         xv.y = xv.y - cx * rv[m].y;
                         pv.x = pv.x + cb * rv[m].x;
@@ -408,6 +431,172 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_flush_kernel(int Vh, int nshift,
     double none[1] = {0.0};
     FinWindow fin{st};
     reduce_finalize<1>(none, partials, ticket, fin);
+}
+
+// ------------------------------------------------------------------ precision-scheduled resumption
+// The rounding error a sloppy iteration adds to the shifted systems is proportional to the
+// residual at that iteration, and the shifted systems never see it corrected (only the base
+// system is reliably updated).  So the mixed solver runs its first iterations in FP64, stops each
+// right-hand side once |r| <= tau |b|, and resumes the same recurrences (same scalars, same
+// shifted vectors) with FP32 base vectors and links: every later error is then tau times smaller.
+
+// One thread: every RHS that has not reached the final target (and still has an active shift)
+// runs again; the phase target becomes the final one and a new window starts.
+static __global__ void ms_rearm_kernel(MSState *st)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int any = 0;
+    for (int r = 0; r < st->nrhs; r++) {
+        MSRhs &q = st->rhs[r];
+        q.res = st->res;
+        int nact = 0;
+        for (int i = 0; i < st->nshift; i++) nact += q.active_next[i];
+        const int go = st->status == 0 && isfinite(q.lambda) && q.b2 > 0.0 && sqrt(q.lambda) > st->res && nact > 0;
+        q.running_next = go;
+        q.ru_best = q.lambda;
+        q.ru_stall = 0;
+        any |= go;
+    }
+    st->tau = 0.0;
+    st->stop = any ? 0 : 1;
+    st->stop_k4 = 0;
+    st->wpos = 0;
+    st->ru_windows = 0;
+    st->ru_now = 0;
+}
+
+// The current residual of every RHS (ring slot rslot of the previous phase) into the last slot of
+// the new ring, and the base direction p, converted to the new phase's precision.
+template <typename Rf, typename Rt, int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) ms_convert_kernel(int Vh, size_t stride, const typename MSVec<Rf>::E *__restrict__ ring_f,
+                                                                const typename MSVec<Rf>::E *__restrict__ p_f,
+                                                                typename MSVec<Rt>::E *ring_t, typename MSVec<Rt>::E *p_t,
+                                                                const MSState *st)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Vh) return;
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        const int slot = st->rhs[j].rslot;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const size_t o = j * stride + (size_t)c * Vh + k;
+            const typename MSVec<Rf>::E rv = ring_f[(size_t)slot * NR * stride + o], pv = p_f[o];
+            typename MSVec<Rt>::E a, b;
+            a.x = (Rt)rv.x;
+            a.y = (Rt)rv.y;
+            b.x = (Rt)pv.x;
+            b.y = (Rt)pv.y;
+            ring_t[(size_t)(MS_WIN - 1) * NR * stride + o] = a;
+            p_t[o] = b;
+        }
+    }
+}
+
+// One thread, after the window's flush: decides whether this window ends with a reliable update.
+static __global__ void ms_ru_begin_kernel(MSState *st)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    st->ru_now = 0;
+    if (st->stop) return;
+    st->ru_windows++;
+    int any = 0;
+    for (int r = 0; r < st->nrhs; r++) any |= st->rhs[r].running_next;
+    st->ru_now = any && (st->ru_windows % st->ru_every == 0);
+}
+
+// x0[j] = x_{j, i0(j)}: the FP64 base solution of every RHS, contiguous for the FP64 operator
+template <int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) ms_gather_base_kernel(int Vh, int nshift, size_t stride, const double2 *__restrict__ x,
+                                                                    double2 *x0, const MSState *st)
+{
+    if (!*(volatile const int *)&st->ru_now) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Vh) return;
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        const size_t src = (size_t)(j * nshift + st->rhs[j].i0) * stride;
+#pragma unroll
+        for (int c = 0; c < 3; c++) x0[j * stride + (size_t)c * Vh + k] = x[src + (size_t)c * Vh + k];
+    }
+}
+
+// A right-hand side whose true base residual has not fallen by 4x (|r| by 2x) over
+// MS_RU_STALL reliable updates, or has grown 4x above its best, has reached the rounding floor
+// of the FP64 operator: past it the sloppy recurrence only follows rounding noise and diverges.
+// It stops there (its solutions as they are) and is left to the refinement that follows.
+constexpr int MS_RU_STALL = 16;
+
+template <int NR>
+struct FinMsRU {
+    MSState *st;
+    __device__ void operator()(const double *tot) const
+    {
+        if (threadIdx.x != 0) return;
+        int any = 0;
+        for (int r = 0; r < NR; r++) {
+            MSRhs &q = st->rhs[r];
+            if (!q.running_next) continue;
+            if (!isfinite(tot[r])) {
+                st->status = 2;
+                q.running_next = 0;
+                continue;
+            }
+            q.delta = tot[r];
+            q.lambda = tot[r];
+            if (tot[r] < 0.25 * q.ru_best) {
+                q.ru_best = tot[r];
+                q.ru_stall = 0;
+            } else if (++q.ru_stall >= MS_RU_STALL || tot[r] > 4.0 * q.ru_best) {
+                q.running_next = 0;
+            }
+            any |= q.running_next;
+        }
+        for (int r = NR; r < st->nrhs; r++) any |= st->rhs[r].running_next;
+        if (!any) st->stop = 1;
+        st->ru_count++;
+    }
+};
+
+// Reliable update of every running RHS: r = b - t with t = (M^dag M + sigma_0) x0 computed in
+// FP64 (the true residual of the base system) replaces the window's last residual, and the
+// base direction is re-synchronised with the FP64 shifted direction of the base shift (both
+// follow the same recurrence; the sloppy copy drifts by rounding).  |r|^2 becomes delta.
+template <typename Rv, int NR>
+__global__ void __launch_bounds__(VEC_BLOCK) ms_ru_resid_kernel(int Vh, int nshift, size_t stride, const double2 *__restrict__ b,
+                                                                 const double2 *__restrict__ t, const double2 *__restrict__ ps,
+                                                                 typename MSVec<Rv>::E *ring, typename MSVec<Rv>::E *p,
+                                                                 double *partials, unsigned *ticket, MSState *st)
+{
+    typedef typename MSVec<Rv>::E E;
+    if (!*(volatile const int *)&st->ru_now) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double red[NR];
+#pragma unroll
+    for (int j = 0; j < NR; j++) red[j] = 0.0;
+    if (k < Vh) {
+#pragma unroll
+        for (int j = 0; j < NR; j++) {
+            if (!st->rhs[j].running_next) continue;
+            const size_t pbase = (size_t)(j * nshift + st->rhs[j].i0) * stride;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const size_t o = j * stride + (size_t)c * Vh + k;
+                const double2 bv = b[o], tv = t[o], pv = ps[pbase + (size_t)c * Vh + k];
+                const double re = bv.x - tv.x, im = bv.y - tv.y;
+                red[j] += re * re + im * im;
+                E e, f;
+                e.x = (Rv)re;
+                e.y = (Rv)im;
+                f.x = (Rv)pv.x;
+                f.y = (Rv)pv.y;
+                ring[(size_t)(MS_WIN - 1) * NR * stride + o] = e;
+                p[o] = f;
+            }
+        }
+    }
+    FinMsRU<NR> fin{st};
+    reduce_finalize<NR>(red, partials, ticket, fin);
 }
 
 }  // namespace rhmc

@@ -35,6 +35,8 @@
 namespace rhmc {
 
 constexpr int RB_MAX = 8;
+// windows (of MS_WIN iterations) between reliable updates of the FP32 multi-shift phase
+constexpr int MX_RU_WINDOWS = 4;
 
 struct ResidCoef {
     double coef[8];  // mass^2 + sigma of each batched system
@@ -253,16 +255,6 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_p_kernel(int Vh, size_t sstride,
     }
 }
 
-template <typename E>
-__global__ void convert_kernel(long n, double2 *dst, const E *src)
-{
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        E v = src[i];
-        dst[i] = make_double2((double)v.x, (double)v.y);
-    }
-}
-
 // ------------------------------------------------------------------ Phase B driver
 template <class LF, int NR>
 static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double *tgt, double2 *xg, const double2 *bg,
@@ -353,16 +345,13 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
         rb_accum_kernel<NR, X><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (X *)xs, st);
-        constexpr int B64 = DslashCfg<L64_18, NR, false>::block, BS1 = DslashCfg<LF, NR, false>::block,
-                      BS2 = DslashCfg<LF, NR, true>::block;
-        const int g64 = grid_for(Vh, B64), gs1 = grid_for(Vh, BS1), gs2 = grid_for(Vh, BS2);
-        dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d1);
-        dslash_kernel<L64_18, NR, false, false, NoFin><<<g64, B64, 0, s_>>>(d2);
+        dslash_launch<L64_18, NR, false, false, NoFin>(d1, Vh, s_);
+        dslash_launch<L64_18, NR, false, false, NoFin>(d2, Vh, s_);
         rb_resid_kernel<NR, S><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, sstride, bg, xg, (const double2 *)t64, (E *)rs, (E *)p,
                                                              co, pt, tk, st);
         for (int it = 0; it < n_ru; it++) {
-            dslash_kernel<LF, NR, false, false, NoFin><<<gs1, BS1, 0, s_>>>(s1);
-            dslash_kernel<LF, NR, true, true, FinRBAlpha<NR>><<<gs2, BS2, 0, s_>>>(s2);
+            dslash_launch<LF, NR, false, false, NoFin>(s1, Vh, s_);
+            dslash_launch<LF, NR, true, true, FinRBAlpha<NR>>(s2, Vh, s_);
             rb_xr_kernel<NR, S, X><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, sstride, (X *)xs, (E *)rs, (const E *)p, (const E *)ap, pt,
                                                              tk + 2, st);
             rb_p_kernel<NR, S><<<gv, VEC_BLOCK, 0, s_>>>(Vh, sstride, (const E *)rs, (E *)p, st);
@@ -375,39 +364,12 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
         c->graphs.put(kb, exec);
     }
 
-    int *hflag = c->hflags;
-    cudaEvent_t ev[2];
-    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
     const long max_rep = max_iter / n_ru + 2;
     long rep = 0;
-    bool done = false;
-    hflag[0] = hflag[1] = 0;
-    const bool dbg = getenv("RHMC_DEBUG") != nullptr;
-    for (; rep < max_rep && !done; rep++) {
-        ce = cudaGraphLaunch(exec, s_);
-        if (ce != cudaSuccess) break;
-        if (dbg) {
-            RBState d;
-            cudaMemcpyAsync(&d, st, sizeof(d), cudaMemcpyDeviceToHost, s_);
-            cudaStreamSynchronize(s_);
-            fprintf(stderr, "[refine n=%d rep=%ld iters=%d ru=%d stop=%d status=%d]", NR, rep, d.iters, d.ru_count, d.stop, d.status);
-            for (int j = 0; j < NR; j++)
-                fprintf(stderr, " (%d%d r2t=%.3e rr=%.3e)", d.conv[j], d.pending[j], d.r2true[j], d.rr[j]);
-            fprintf(stderr, "\n");
-        }
-        cudaMemcpyAsync(&hflag[rep & 1], &st->stop, sizeof(int), cudaMemcpyDeviceToHost, s_);
-        cudaEventRecord(ev[rep & 1], s_);
-        if (rep >= 1) {
-            cudaEventSynchronize(ev[(rep - 1) & 1]);
-            if (hflag[(rep - 1) & 1]) done = true;
-        }
-    }
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s_);
+    int seen = 0;
+    const int prc = replay_until_stop(c, exec, s_, &st->stop, max_rep, &rep, &seen, "refine loop");
     c->launches += rep * (4 + 4 * (long)n_ru);
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
-    if (ce != cudaSuccess) return cuda_fail(ce, "refine loop");
+    if (prc) return prc;
     RBState hs;
     CK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
     *iters_out += hs.iters;
@@ -479,7 +441,6 @@ static int refine_all(rhmc_ctx *c, const LF &lf, int nshift, const double *shift
 int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrhs, double res, int max_iter, double tolA,
                  double ru_delta, double2 *x, const double2 *b, rhmc_msolve_info *info)
 {
-    const size_t stride = 3 * (size_t)c->Vh;
     auto t0 = std::chrono::steady_clock::now();
     std::vector<double> base(nrhs);  // each RHS iterates on its smallest pole
     for (int r = 0; r < nrhs; r++) {
@@ -498,7 +459,8 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
     MSolveInfo mi;
     memset(&mi, 0, sizeof(mi));
     std::vector<double> tgt(nshift);
-    std::vector<double> tr;  // FP64 true residuals after phase A (FP64 phase A only)
+    std::vector<double> tr;  // FP64 true residuals after the multi-shift phase
+    int it_hi[8] = {0};      // iterations of each RHS in the FP64 part of the precision schedule
     int rc;
     const bool f64a = fmt_is_f64(fmt);
     if (f64a) {
@@ -514,32 +476,29 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
         if (rc) return rc;
         for (double &v : tr) v = std::sqrt(v);
     } else {
-        // Phase A in FP32 to tol_A |b|, then every system is refined
-        std::vector<double> b2(nrhs);
-        void *z;
-        CK(c->ws.get("mx_zero", stride * sizeof(double2), &z));
-        CK(cudaMemsetAsync(z, 0, stride * sizeof(double2), c->stream));
-        const double s0 = 0.0;
-        for (int r = 0; r < nrhs; r++) {
-            rc = true_residuals(c, 1, &s0, 1, (const double2 *)z, b + r * stride, &b2[r]);
-            if (rc) return rc;
-        }
-        double bmax = 0;
-        for (double v : b2) bmax = std::max(bmax, std::sqrt(v));
-        for (double &t : tgt) t = std::max(res, tolA * bmax);
-        void *xa;
-        CK(c->ws.get("mx_xa", (size_t)nrhs * nshift * stride * sizeof(float2), &xa));
+        // Precision schedule: FP64 (12-real links) until |r| <= tol_A |b| for every RHS, then the
+        // same recurrences resumed with FP32 links and base vectors, FP64 shifted vectors and a
+        // reliable update of the base system every MX_RU_WINDOWS windows, to the final target.
+        for (double &t : tgt) t = res;
         A.tgt = tgt.data();
-        A.res_base = std::max(res, tolA * bmax);
-        A.x = xa;
-        // half refinement follows an FP32 multi-shift on 12-real links
-        rc = msolve_shifted(c, fmt == RHMC_LINKS_F16_12 ? RHMC_LINKS_F32_12 : fmt, A, &mi);
+        A.res_base = res;
+        A.x = x;
+        A.tau = tolA;
+        rc = msolve_shifted(c, RHMC_LINKS_F64_12, A, &mi);
         if (rc && rc != RHMC_ERR_MAXITER) return rc;
-        const long n = (long)nrhs * nshift * stride;
-        convert_kernel<float2><<<grid_for(n, 256), 256, 0, c->stream>>>(n, x, (const float2 *)xa);
-        c->launches++;
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(c->stream));
+        for (int r = 0; r < nrhs && r < 8; r++) it_hi[r] = mi.iters[r];
+        if (rc == RHMC_OK) {
+            A.fresh = 0;
+            A.tau = 0.0;
+            A.ru_every = MX_RU_WINDOWS;
+            // half refinement follows an FP32 multi-shift on 12-real links
+            rc = msolve_shifted(c, fmt == RHMC_LINKS_F16_12 ? RHMC_LINKS_F32_12 : fmt, A, &mi);
+            if (rc && rc != RHMC_ERR_MAXITER) return rc;
+        }
+        tr.resize((size_t)nshift * nrhs);
+        rc = true_residuals(c, nshift, shifts, nrhs, x, b, tr.data());
+        if (rc) return rc;
+        for (double &v : tr) v = std::sqrt(v);
     }
     const double t_a = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     long it_b = 0;
@@ -548,7 +507,8 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
     if (fmt == RHMC_LINKS_F16_12) {
         L16_12 lf;
         links_f16_12(c, &lf);
-        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX, nullptr, &nsys);
+        rc = refine_all(c, lf, nshift, shifts, nrhs, res, max_iter, x, b, &it_b, &ru, ru_delta, RB_MAX,
+                        tr.empty() ? nullptr : tr.data(), &nsys);
     } else if (fmt == RHMC_LINKS_F32_18 || fmt == RHMC_LINKS_F64_18) {
         L32_18 lf;
         links_f32_18(c, &lf);
@@ -569,6 +529,8 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
         info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         info->seconds_phase_a = t_a;
         info->systems_refined = nsys;
+        for (int r = 0; r < nrhs && r < 8; r++) info->iters_fp64 += f64a ? mi.iters[r] : it_hi[r];
+        info->ms_reliable_updates = f64a ? 0 : mi.ru_count;
     }
     return rc;
 }
@@ -576,6 +538,18 @@ int msolve_mixed(rhmc_ctx *c, int fmt, int nshift, const double *shifts, int nrh
 }  // namespace rhmc
 
 using namespace rhmc;
+
+// multi-shift iteration counts of right-hand sides first..first+n-1 into info (the per-RHS
+// array holds the first 8; the total and the maximum cover all of them)
+static void add_iters(rhmc_msolve_info *info, int first, const int *it, int n)
+{
+    if (!info) return;
+    for (int j = 0; j < n; j++) {
+        if (first + j < 8) info->iters[first + j] = it[j];
+        info->iters_total += it[j];
+        if (it[j] > info->iters_max) info->iters_max = it[j];
+    }
+}
 
 // sh: the pole sets [nrhs][nshift]
 static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, const double *sh, double2 *x, const double2 *b,
@@ -603,8 +577,7 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, const double *s
         MSolveInfo mi;
         memset(&mi, 0, sizeof(mi));
         rc = msolve_shifted(c, P->fmt, A, &mi);
-        if (info)
-            for (int j = 0; j < n && done + j < 8; j++) info->iters[done + j] = mi.iters[j];
+        add_iters(info, done, mi.iters, n);
         if (rc) break;
         done += n;
     }
@@ -636,7 +609,9 @@ static int msolve_fp64(rhmc_ctx *c, const rhmc_msolve_params *P, const double *s
 }
 
 // The reference's single-precision path (cuda_shifted_inverter, lib/Cuda/cuda_inverter.cu:647-857):
-// the same recurrences with FP32 links and vectors, FP64 scalars; solutions returned in FP64.
+// the same recurrences with FP32 links and base vectors and FP64 scalars.  The shifted solutions
+// and directions are accumulated in FP64 (the reference keeps them in FP32), which removes their
+// storage rounding from the true residual; they are written straight into x.
 static int msolve_fp32(rhmc_ctx *c, const rhmc_msolve_params *P, const double *sh, double2 *x, const double2 *b,
                        rhmc_msolve_info *info)
 {
@@ -644,8 +619,6 @@ static int msolve_fp32(rhmc_ctx *c, const rhmc_msolve_params *P, const double *s
     std::vector<double> tgt(P->nshift, P->residual), zero(MS_MAX_RHS, 0.0);
     auto t0 = std::chrono::steady_clock::now();
     int done = 0, rc = RHMC_OK;
-    void *xa;
-    CK(c->ws.get("mx_xa", (size_t)8 * P->nshift * stride * sizeof(float2), &xa));
     while (done < P->nrhs) {
         const int left = P->nrhs - done;
         const int n = left >= 8 ? 8 : (left >= 4 ? 4 : left);
@@ -660,17 +633,12 @@ static int msolve_fp32(rhmc_ctx *c, const rhmc_msolve_params *P, const double *s
         A.stop_on_frozen = 1;
         A.chunk = 8;
         A.b = b + (size_t)done * stride;
-        A.x = xa;
+        A.x = x + (size_t)done * P->nshift * stride;
         MSolveInfo mi;
         memset(&mi, 0, sizeof(mi));
         rc = msolve_shifted(c, P->fmt, A, &mi);
-        if (info)
-            for (int j = 0; j < n && done + j < 8; j++) info->iters[done + j] = mi.iters[j];
+        add_iters(info, done, mi.iters, n);
         if (rc) break;
-        const long nel = (long)n * P->nshift * stride;
-        convert_kernel<float2><<<grid_for(nel, 256), 256, 0, c->stream>>>(nel, x + (size_t)done * P->nshift * stride, (const float2 *)xa);
-        c->launches++;
-        CK(cudaGetLastError());
         done += n;
     }
     CK(cudaStreamSynchronize(c->stream));
@@ -707,7 +675,7 @@ int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const doubl
     }
     if (P->mode == RHMC_MSOLVE_MIXED) {
         if (P->fmt < 0 || P->fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad link format %d", P->fmt);
-        const double tolA = P->tol_phase_a > 0 ? P->tol_phase_a : 3e-6;
+        const double tolA = P->tol_phase_a > 0 ? P->tol_phase_a : 1e-3;
         const double rud = (P->ru_delta > 0 && P->ru_delta < 1) ? P->ru_delta : 0.05;
         // batches of 8, 4, 3, 2 or 1 right-hand sides (the widths the kernels are built for)
         const size_t stride = 3 * (size_t)c->Vh;
@@ -720,12 +688,14 @@ int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const doubl
             memset(&part, 0, sizeof(part));
             rc = msolve_mixed(c, P->fmt, P->nshift, sh.data() + (size_t)done * P->nshift, n, P->residual, P->max_iter, tolA, rud,
                               (double2 *)x + (size_t)done * P->nshift * stride, (const double2 *)b + (size_t)done * stride, &part);
-            for (int j = 0; j < n && done + j < 8; j++) agg.iters[done + j] = part.iters[j];
+            add_iters(&agg, done, part.iters, n);
             agg.refine_iters += part.refine_iters;
             agg.reliable_updates += part.reliable_updates;
             agg.seconds += part.seconds;
             agg.seconds_phase_a += part.seconds_phase_a;
             agg.systems_refined += part.systems_refined;
+            agg.iters_fp64 += part.iters_fp64;
+            agg.ms_reliable_updates += part.ms_reliable_updates;
             done += n;
         }
         agg.status = rc;

@@ -14,6 +14,7 @@
 //                                      consecutive spinors (stride 3*Vh elements)
 //   algebra  [mu][parity][8][Vh]      reals: traceless (anti-)hermitian matrices
 #pragma once
+#include <cfloat>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -431,6 +432,9 @@ struct H16S {
         float m = 0.f;
 #pragma unroll
         for (int c = 0; c < 3; c++) m = fmaxf(m, fmaxf(fabsf((float)r.c[c].re), fabsf((float)r.c[c].im)));
+        // a site whose largest component is below the smallest normal float is stored as zero:
+        // 1/m would overflow to inf there and turn the halves into inf or NaN
+        if (!(m >= FLT_MIN)) m = 0.f;
         const float inv = m > 0.f ? 1.f / m : 0.f;
         uint4 q;
         q.x = f2h((float)r.c[0].re * inv, (float)r.c[0].im * inv);

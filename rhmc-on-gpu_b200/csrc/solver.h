@@ -16,7 +16,10 @@ struct MSolveArgs {
     int stop_on_frozen;
     int chunk;            // iterations per captured graph (the multi-shift loop uses its window, MS_WIN)
     const void *b;        // FP64 internal spinors, nrhs of them
-    void *x;              // internal spinors of the link format's precision, [nrhs][nshift]
+    void *x;              // FP64 internal spinors, [nrhs][nshift]
+    int fresh = 1;        // 1: start from x = 0; 0: resume the state an FP64 phase left (FP32 links only)
+    double tau = 0.0;     // > 0: stop each RHS once |r| <= tau |b| (to be resumed in lower precision)
+    int ru_every = 0;     // > 0: reliable update of the base system every ru_every windows
 };
 
 struct MSolveInfo {
@@ -25,7 +28,16 @@ struct MSolveInfo {
     int iters[8];
     double lambda[8];
     double b2[8];
+    int ru_count;
 };
+
+// Replays `exec` on stream s until the device word *stop is non-zero (read one replay behind
+// through a pinned host word, so the GPU never idles on the poll) or max_rep replays.
+// *replays receives the number of replays issued.  Every CUDA call is checked: a failure
+// returns RHMC_ERR_CUDA with the stream synchronised, and a loop that ends before the flag is
+// seen leaves *stop_seen = 0.
+int replay_until_stop(rhmc_ctx *c, cudaGraphExec_t exec, cudaStream_t s, const int *stop, long max_rep, long *replays,
+                      int *stop_seen, const char *what);
 
 // Multi-shift CG with links of format `fmt`; vectors in that format's precision.
 int msolve_shifted(rhmc_ctx *c, int fmt, const MSolveArgs &A, MSolveInfo *info);

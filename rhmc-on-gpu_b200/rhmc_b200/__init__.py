@@ -212,12 +212,15 @@ class MsolveParams(ctypes.Structure):
 class MsolveInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("iters", ctypes.c_int * 8), ("refine_iters", ctypes.c_long),
                 ("reliable_updates", ctypes.c_int), ("seconds", ctypes.c_double), ("seconds_phase_a", ctypes.c_double),
-                ("systems_refined", ctypes.c_int)]
+                ("systems_refined", ctypes.c_int), ("iters_total", ctypes.c_long), ("iters_max", ctypes.c_int),
+                ("iters_fp64", ctypes.c_long), ("ms_reliable_updates", ctypes.c_int)]
 
     def as_dict(self):
         return {"status": self.status, "iters": list(self.iters), "refine_iters": self.refine_iters,
                 "reliable_updates": self.reliable_updates, "seconds": self.seconds,
-                "seconds_phase_a": self.seconds_phase_a, "systems_refined": self.systems_refined}
+                "seconds_phase_a": self.seconds_phase_a, "systems_refined": self.systems_refined,
+                "iters_total": self.iters_total, "iters_max": self.iters_max, "iters_fp64": self.iters_fp64,
+                "ms_reliable_updates": self.ms_reliable_updates}
 
 
 def _msolve_params(shifts, nrhs, residual, max_iter, mode, fmt, tol_phase_a=0.0, certify=0, ru_delta=0.0):

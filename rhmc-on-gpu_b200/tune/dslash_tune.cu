@@ -1,13 +1,15 @@
-// dslash_tune.cu -- offline tuner of the Dslash launch configurations (DslashCfg in
+// dslash_tune.cu -- offline sweep of the Dslash launch configurations (DslashCfg in
 // csrc/dslash.cuh).  For the link formats and RHS counts the solvers launch, it times the
 // half-Dslash kernel with and without the fused reductions for a set of (threads per block,
 // minimum resident blocks per SM) pairs, with CUDA events over 20 back-to-back launches after 3
 // warm-ups, and prints registers, spills, resident blocks and GB/s of algorithmic traffic.
 // DslashCfg encodes the fastest pair of each case.  Inputs are deterministic patterns (the
 // timing does not depend on the values).
-//   make -C rhmc-on-gpu_b200 tune && rhmc-on-gpu_b200/_build/dslash_tune 32 32
+//   make -C rhmc-on-gpu_b200 tune && rhmc-on-gpu_b200/_build/dslash_tune 32 32 [filter]
+// filter: run only the cases whose "<format> NR=<n> red=<0|1>" label contains it.
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 #include "../csrc/dslash.cuh"
 using namespace rhmc;
@@ -20,45 +22,48 @@ static Geom G;
 static void *Ubuf, *In, *Out, *Y, *Part;
 static unsigned *Tick;
 static cudaEvent_t e0, e1;
+static const char *Filter = nullptr;
 
 template <class LF, int NR, bool RED, int B, int MB>
 void timeit(const char *lname, LF lf)
 {
     typedef typename LF::real R;
-    typedef typename SpinorT<R>::elem E;
+    typedef typename LF::store::elem E;
     DslashArgs<LF, NR, NoFin> a;
     memset(&a, 0, sizeof(a));
     a.g = G; a.p_out = 1; a.links = lf; a.in = (const E *)In; a.out = (E *)Out; a.y = RED ? (const E *)Y : nullptr;
-    a.stride = 3 * (size_t)G.Vh; a.alpha = (R)0.01; a.beta = (R)-0.5; a.use_alphas = 0;
+    a.stride = (size_t)LF::store::planes * G.Vh; a.alpha = (R)0.01; a.beta = (R)-0.5; a.use_alphas = 0;
     for (int r = 0; r < NR; r++) a.alphas[r] = (R)0.01;
     a.partials = (double *)Part; a.ticket = Tick;
-    const int grid = (G.Vh + B - 1) / B;
+    auto kern = dslash_kernel<LF, NR, RED, RED, NoFin, B, MB>;
     cudaFuncAttributes fa;
-    cudaFuncGetAttributes(&fa, dslash_kernel<LF, NR, RED, RED, NoFin, B, MB>);
+    cudaFuncGetAttributes(&fa, kern);
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, dslash_kernel<LF, NR, RED, RED, NoFin, B, MB>, B, 0);
-    for (int i = 0; i < 3; i++) dslash_kernel<LF, NR, RED, RED, NoFin, B, MB><<<grid, B>>>(a);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, B, 0);
+    for (int i = 0; i < 3; i++) CKE((dslash_launch<LF, NR, RED, RED, NoFin, B, MB>(a, G.Vh, 0)));
     CKE(cudaDeviceSynchronize());
     const int REP = 20;
     cudaEventRecord(e0);
-    for (int i = 0; i < REP; i++) dslash_kernel<LF, NR, RED, RED, NoFin, B, MB><<<grid, B>>>(a);
+    for (int i = 0; i < REP; i++) dslash_launch<LF, NR, RED, RED, NoFin, B, MB>(a, G.Vh, 0);
     cudaEventRecord(e1);
     CKE(cudaEventSynchronize(e1));
     float ms;
     cudaEventElapsedTime(&ms, e0, e1);
     ms /= REP;
-    const double ws = sizeof(R);
-    const double bytes = (double)G.Vh * (8.0 * LF::reals * ws + NR * (12.0 + (RED ? 6.0 : 0.0)) * ws);
-    printf("%-7s NR=%d red=%d block=%3d minb=%d regs=%3d spill=%4d blocks/SM=%d  %8.1f us  %7.1f GB/s\n", lname, NR, (int)RED, B, MB,
-           fa.numRegs, (int)fa.localSizeBytes, nb, ms * 1e3, bytes / (ms * 1e-3) / 1e9);
+    const double ws = LF::store::planes == 1 ? 16.0 / 6.0 : sizeof(typename LF::store::real);  // bytes per spinor real
+    const double bytes = (double)G.Vh * (8.0 * LF::bytes + NR * (12.0 + (RED ? 6.0 : 0.0)) * ws);
+    printf("%-7s NR=%d red=%d block=%3d minb=%d regs=%3d spill=%4d blocks/SM=%d  %8.1f us  %7.1f GB/s\n", lname, NR,
+           (int)RED, B, MB, fa.numRegs, (int)fa.localSizeBytes, nb, ms * 1e3, bytes / (ms * 1e-3) / 1e9);
 }
 
 template <class LF, int NR, bool RED>
 void sweep(const char *n, LF lf)
 {
+    char label[64];
+    snprintf(label, sizeof(label), "%s NR=%d red=%d", n, NR, (int)RED);
+    if (Filter && !strstr(label, Filter)) return;
     timeit<LF, NR, RED, 256, 1>(n, lf);
     timeit<LF, NR, RED, 256, 2>(n, lf);
-    timeit<LF, NR, RED, 256, 3>(n, lf);
     timeit<LF, NR, RED, 128, 2>(n, lf);
     timeit<LF, NR, RED, 128, 3>(n, lf);
     timeit<LF, NR, RED, 128, 4>(n, lf);
@@ -69,6 +74,7 @@ void sweep(const char *n, LF lf)
 int main(int argc, char **argv)
 {
     const int nx = argc > 1 ? atoi(argv[1]) : 32, nt = argc > 2 ? atoi(argv[2]) : 32;
+    Filter = argc > 3 ? argv[3] : nullptr;
     G = Geom{nx, nx, nx, nt, nx * nx * nx * nt / 2, 1};
     const long Vh = G.Vh;
     printf("lattice %d^3x%d Vh=%ld\n", nx, nt, Vh);
@@ -89,14 +95,23 @@ int main(int argc, char **argv)
     L64_18 l18; l18.p = (const double2 *)Ubuf; l18.Vh = (int)Vh;
     L64_12 l12; l12.p = (const double2 *)Ubuf; l12.Vh = (int)Vh;
     L32_12 f12; f12.p = (const float4 *)Ubuf; f12.Vh = (int)Vh;
+    L32_18 f18; f18.p = (const float4 *)Ubuf; f18.Vh = (int)Vh;
+    L16_12 h12; h12.p = (const uint4 *)Ubuf; h12.Vh = (int)Vh;
     sweep<L64_18, 1, false>("f64_18", l18);
     sweep<L64_18, 1, true>("f64_18", l18);
+    sweep<L64_12, 1, false>("f64_12", l12);
     sweep<L64_12, 4, false>("f64_12", l12);
     sweep<L64_12, 4, true>("f64_12", l12);
     sweep<L64_18, 8, false>("f64_18", l18);
+    sweep<L32_12, 1, false>("f32_12", f12);
+    sweep<L32_12, 4, false>("f32_12", f12);
+    sweep<L32_12, 4, true>("f32_12", f12);
     sweep<L32_12, 8, false>("f32_12", f12);
     sweep<L32_12, 8, true>("f32_12", f12);
-    sweep<L32_12, 4, true>("f32_12", f12);
+    sweep<L32_18, 1, false>("f32_18", f18);
+    sweep<L16_12, 1, false>("f16_12", h12);
+    sweep<L16_12, 8, false>("f16_12", h12);
+    sweep<L16_12, 8, true>("f16_12", h12);
     CKE(cudaGetLastError());
     return 0;
 }

@@ -158,3 +158,24 @@ def test_half_spinor_roundtrip():
     site_max = np.maximum(np.abs(x.real), np.abs(x.imag)).max(1)
     err = np.maximum(np.abs((back - x).real), np.abs((back - x).imag)).max(1)
     assert np.all(err <= site_max * 2.0 ** -11 * 1.01)
+
+
+def test_half_spinor_tiny_sites_flush_to_zero():
+    """Sites whose largest component is below the smallest normal float (1/scale would overflow)
+    are stored as zero instead of inf/NaN; the Dslash of such a field stays finite."""
+    from gpu_util import new_ctx, to_internal, from_internal, internal_buffer
+    dims = (6, 4, 4, 8)
+    ctx = new_ctx(dims)
+    ctx.set_gauge(F.random_links(dims, seed=10))
+    x = F.random_spinor(dims, seed=11)
+    tiny = np.arange(ctx.Vh) % 3 == 0
+    x[tiny] *= 1e-40
+    xin = to_internal(ctx, rb.LINKS_F16_12, x)
+    back = from_internal(ctx, rb.LINKS_F16_12, xin)
+    assert np.all(np.isfinite(back))
+    assert not np.any(back[tiny])
+    normal = ~tiny
+    assert rel_err(back[normal], x[normal]) < 2e-3
+    out = internal_buffer(ctx, rb.LINKS_F16_12)
+    ctx.dslash(rb.LINKS_F16_12, 1, out, xin)
+    assert np.all(np.isfinite(from_internal(ctx, rb.LINKS_F16_12, out)))

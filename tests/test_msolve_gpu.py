@@ -91,6 +91,11 @@ def test_msolve_mixed_true_residual(fmt, nrhs, oracle_mod):
     res = 1e-10
     xm, info = ctx.msolve_host(bs if nrhs > 1 else bs[0], shifts, res, mode=rb.MSOLVE_MIXED, fmt=fmt)
     assert info["status"] == 0, info
+    # the precision schedule handed over to FP32 with reliable updates, and left at most a few
+    # systems for the refinement
+    assert 0 < info["iters_fp64"] < info["iters_total"], info
+    assert info["ms_reliable_updates"] > 0, info
+    assert info["systems_refined"] <= 2 * nrhs, info
     xm = xm.reshape(nrhs, len(shifts), ctx.Vh, 3)
     # FP64 true residuals through the library and through the oracle operator
     orc = oracle_mod.Oracle(dims)
