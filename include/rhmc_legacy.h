@@ -77,6 +77,9 @@ void cuda_momenta_sum_multiply(float step);
 /* lib/Cuda/cuda_find_min_max.h:6-7 (REAL = double, include/global_macro.h:5) */
 void cuda_find_max(double *max);
 void cuda_find_min(double *min, const double max);
+/* lib/Cuda/DeviceInfo/device_info.h:4-6 (called by lib/Main/rhmc.cc:318): selects the device and
+ * prints its properties. */
+void GPUDeviceInfo(const int gpu_device);
 
 /* The power iterations behind cuda_find_max/min through the handle API (FP64): start is a
  * host spinor in the reference layout; stops when the relative change is below 5e-4

@@ -565,4 +565,21 @@ void cuda_find_min(double *min, const double max)
     if (rhmc_find_min(g_ctx, s.data(), max, min) != RHMC_OK) die("cuda_find_min");
 }
 
+// GPUDeviceInfo (lib/Cuda/DeviceInfo/device_info.h:4-6), which the reference's main program calls
+// once at start-up: selects the device and prints its properties; exits when it does not exist.
+void GPUDeviceInfo(const int gpu_device)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || gpu_device < 0 || gpu_device >= n) {
+        fprintf(stderr, "librhmc_b200 GPUDeviceInfo: device %d not available (%d CUDA devices)\n", gpu_device, n);
+        exit(-1);
+    }
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, gpu_device) != cudaSuccess || cudaSetDevice(gpu_device) != cudaSuccess) die("GPUDeviceInfo");
+    printf("device %d: %s, compute capability %d.%d, %d SMs, %.1f GB global memory, %.1f MB L2, %zu KB shared memory "
+           "per block (opt-in), clock %.0f MHz\n",
+           gpu_device, p.name, p.major, p.minor, p.multiProcessorCount, p.totalGlobalMem / 1e9, p.l2CacheSize / 1e6,
+           p.sharedMemPerBlockOptin / 1024, p.clockRate / 1e3);
+}
+
 }  // extern "C"
