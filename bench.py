@@ -2,11 +2,14 @@
 """Benchmark of the RHMC hot path on B200.
 
 Headline workload: the even/odd staggered Dslash on a 32^4 lattice (Haar-random SU(3) links,
-unit-variance Gaussian spinors, fixed seeds; synthetic data).  One step = one full Dslash,
-D_oe then D_eo (two half-Dslash launches), with FP64 links (18 reals) and FP64 spinors.
-`value` is the algorithmic HBM traffic of those launches per second (GB/s, whole job over all
-ranks); the other link formats are reported under `variants`.  The 32^4 FP64 links (604 MB)
-are larger than the 126 MB L2, so no L2 flush is needed between steps.
+unit-variance Gaussian spinors, fixed seeds; synthetic data).  One step = the 1000 half-Dslash
+applications of the Dslash benchmark configuration: 500 full Dslash, D_oe then D_eo, with FP64
+links (18 reals) and FP64 spinors, each output the next input (after a few hundred applications
+the values overflow; the kernel's time does not depend on them, and its output is checked
+against the reference's Deo/Doe at this lattice by tests/test_dslash32_gpu.py).  `value` is
+the algorithmic HBM traffic of those launches per second (GB/s, whole job over all ranks); the
+other link formats are reported under `variants`.  The 32^4 FP64 links (604 MB) are larger
+than the 126 MB L2, so no L2 flush is needed between steps.
 
 Multi-GPU: independent replicas (the path has no data exchange), one process per GPU,
 "scaling": "weak", value = sum over ranks of the per-rank work / max over ranks of the time.
@@ -27,7 +30,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "rhmc-on-gpu_b200"))
 
 DIMS = (32, 32, 32, 32)
-METRIC = "multi-shift CG s/solve @1e-10 & Dslash GB/s at 32^4: mixed+batched vs plain FP64"
+PAIRS = 500  # full Dslash (D_oe, D_eo) per step: 1000 half-Dslash applications
+METRIC ="multi-shift CG s/solve @1e-10 & Dslash GB/s at 32^4: mixed+batched vs plain FP64"
 
 # algorithmic bytes per output site of one half-Dslash: 8 links + 1 input + 1 output spinor
 LINK_BYTES = {0: 144, 1: 96, 2: 72, 3: 48, 4: 24}
@@ -37,6 +41,18 @@ FLOPS_PER_SITE = 570
 
 def half_dslash_bytes(fmt, Vh, nrhs=1):
     return Vh * (8 * LINK_BYTES[fmt] + 2 * SPINOR_BYTES[fmt] * nrhs)
+
+
+def tuned_shapes(rb, Vh):
+    """The launch shape (threads per block, minimum blocks per SM) the autotuner chose for each
+    Dslash instantiation timed at this volume, with the candidates' times in microseconds."""
+    out = {}
+    for e in rb.tune_report().get("entries", []):
+        dev, vh, what = (e["key"].split("|") + ["", ""])[:3]
+        if vh == "vh=%d" % Vh and what.startswith("dslash"):
+            out[what] = {"block": e["shapes"][e["choice"]][0], "min_blocks": e["shapes"][e["choice"]][1],
+                         "candidates_us": dict(("%dx%d" % tuple(s), t) for s, t in zip(e["shapes"], e["us"]))}
+    return out
 
 
 def load_peaks():
@@ -702,8 +718,8 @@ def rhmc4_bench(a, rb, F, np, torch, rank, dev, stream):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dims", default="32,32,32,32")
@@ -835,7 +851,7 @@ def main():
         ev1 = torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             ev0.record(stream)
-            ctx.dslash_repeat(fmt, xe, xo, 1, a.steps)  # steps x (D_oe, D_eo) issued from C
+            ctx.dslash_repeat(fmt, xe, xo, 1, a.steps * PAIRS)  # steps x PAIRS x (D_oe, D_eo) issued from C
             ev1.record(stream)
         stream.synchronize()
         torch.cuda.synchronize()
@@ -843,14 +859,14 @@ def main():
         launches = ctx.launch_count() - n0
         cl = clocks.stop() if clocks else None
         total_ms = ev0.elapsed_time(ev1)
-        per_launch = [total_ms / (2 * a.steps)]
+        per_launch = [total_ms / (2 * PAIRS * a.steps)]
         total_ms = max_over_ranks(total_ms)
         by_launch = half_dslash_bytes(fmt, Vh)
         avg_launch_ms = sum(per_launch) / len(per_launch)
         results[fmt] = dict(total_ms=total_ms, avg_launch_ms=avg_launch_ms, launches=launches, clocks=cl,
-                            gbs=world * 2 * by_launch * a.steps / (total_ms * 1e-3) / 1e9,
+                            gbs=world * 2 * PAIRS * by_launch * a.steps / (total_ms * 1e-3) / 1e9,
                             achieved=by_launch / (avg_launch_ms * 1e-3) / 1e9,
-                            gflops=world * 2 * FLOPS_PER_SITE * Vh * a.steps / (total_ms * 1e-3) / 1e9)
+                            gflops=world * 2 * PAIRS * FLOPS_PER_SITE * Vh * a.steps / (total_ms * 1e-3) / 1e9)
         del xe, xo
 
     # end to end: reference-facing host call (host spinors in/out, copies inside the timing)
@@ -900,7 +916,9 @@ def main():
             "data": "synthetic (Haar links seed 1001+rank, Gaussian spinor seed 2002+rank)",
             "config": {"workload": "Dslash D_oe+D_eo 32^4 FP64 links(18 real) + FP64 spinors, 1 RHS",
                        "lattice": list(DIMS), "parallelism": "replicas%d" % world,
-                       "l2": "inputs larger than L2 (links 604 MB)"},
+                       "half_dslash_per_step": 2 * PAIRS,
+                       "l2": "inputs larger than L2 (links 604 MB)",
+                       "launch_shapes": tuned_shapes(rb, Vh)},
             "roofline": {"bound": "hbm", "achieved": round(r["achieved"], 1), "peak": peak, "unit": "GB/s",
                          "frac": round(r["achieved"] / peak, 4), "traffic": round(DSLASH_F64_18_DRAM_PER_SITE * Vh),
                          "traffic_note": "ncu dram read+write of this kernel at 24^4 (1244.8 B per output site), "
@@ -911,7 +929,7 @@ def main():
             "variants": {rb.FMT_NAMES[f]: {"gbs": round(v["gbs"], 1), "achieved": round(v["achieved"], 1),
                                             "frac": round(v["achieved"] / peak, 4),
                                             "us_per_half_dslash": round(1000 * v["avg_launch_ms"], 2),
-                                            "sites_per_s": round(2 * Vh * a.steps / (v["total_ms"] * 1e-3) * world, 1)}
+                                            "sites_per_s": round(2 * PAIRS * Vh * a.steps / (v["total_ms"] * 1e-3) * world, 1)}
                          for f, v in results.items()},
             "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s", "h2d_bytes_per_step": 2 * 48 * Vh,
                     "d2h_bytes_per_step": 2 * 48 * Vh, "api": "rhmc_dslash_host (host spinors, pinned)"},

@@ -320,6 +320,31 @@ int rhmc_driver_stats(rhmc_ctx *ctx, long *force_evals, long *solves);
  * events): the compute roofline of the FP64 gauge force and link exponentiation. */
 int rhmc_fma_peak(rhmc_ctx *ctx, int fp64, double *tflops);
 
+/* ------------------------------------------------------------------ launch-configuration autotuner
+ * No counterpart in the reference (it fixes 128 threads per block, include/global_macro.h:8).
+ * Every Dslash instantiation is built in three launch shapes (threads per block, minimum resident
+ * blocks per SM; shape 0 is the compiled-in default).  The first launch of an instantiation on a
+ * device at a volume, outside a stream capture, times the three on scratch spinors with CUDA
+ * events and keeps the fastest; the solvers look their shapes up before capturing their graphs.
+ * Dslash calls with n >= 5 right-hand sides likewise time their RHS packings (launches of at most
+ * 8, 4 or 3 right-hand sides).  Choices are keyed by device name, volume and kernel.  The shapes
+ * change no arithmetic: results are bit-identical whichever shape runs. */
+/* Turns tuning on (default; RHMC_AUTOTUNE=0 in the environment starts with it off) or off (every
+ * launch uses shape 0 and the default packing).  Returns the previous setting. */
+int rhmc_autotune(int enable);
+/* candidate >= 0: every tuned launch uses that candidate (0..2) instead of the tuned choice;
+ * -1: tuned choices again.  Returns the previous value.  For tests and diagnostics. */
+int rhmc_autotune_override(int candidate);
+/* JSON cache of the choices: load merges the entries of `path` (a missing file is an empty cache)
+ * and makes it the file every new choice is saved to; save writes the table to `path` (NULL: the
+ * cache file).  The environment variable RHMC_TUNE_CACHE names a cache file loaded at first use. */
+int rhmc_tune_cache_load(const char *path);
+int rhmc_tune_cache_save(const char *path);
+/* The table as JSON into buf (at most len bytes, NUL-terminated); returns the length needed. */
+long rhmc_tune_report(char *buf, long len);
+/* Forgets every choice (the next launches tune again). */
+int rhmc_tune_clear(void);
+
 /* No counterpart in the reference.  The same values as rhmc_true_residuals, for callers that
  * must not allocate device memory where they check their solutions: programs whose own pool
  * owns all device memory after start-up, chains sharing a GPU under a fixed memory budget, and

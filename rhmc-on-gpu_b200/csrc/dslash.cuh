@@ -13,6 +13,10 @@
 // Re<y, out> in FP64 (the <p, A p> of CG) through reduce_finalize, whose fixed summation order
 // makes results reproducible.
 #pragma once
+#include <cstring>
+#include <string>
+
+#include "autotune.h"
 #include "rhmc_core.cuh"
 
 namespace rhmc {
@@ -144,12 +148,121 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
     if (RED) reduce_finalize<NR>(red, a.partials, a.ticket, a.fin);
 }
 
-// One launch over `nsites` output sites (from a.k_lo) on stream s.
-template <class LF, int NR, bool HAS_Y, bool RED, class FIN, int BLOCK = DslashCfg<LF, NR, RED>::block,
-          int MINB = DslashCfg<LF, NR, RED>::minb>
+// ------------------------------------------------------------------ launch shapes (autotune.h)
+// Candidate 0 is DslashCfg's default; 1 and 2 are the two alternatives the offline sweep found
+// closest for that class of instantiation (all of 128 or 256 threads, as the reductions need).
+template <class LF, int NR, bool RED>
+struct DsCand {
+    typedef DslashCfg<LF, NR, RED> C;
+    static constexpr int b0 = C::block, m0 = C::minb;
+    static constexpr bool def256 = b0 == 256, def1283 = b0 == 128 && m0 == 3;
+    static constexpr int b1 = def256 ? 128 : 256, m1 = def256 ? 4 : (def1283 ? 2 : 1);
+    static constexpr int b2 = 128, m2 = def256 ? 3 : (def1283 ? 4 : 3);
+};
+
+template <class LF, int NR, bool HAS_Y, bool RED, class FIN>
+inline void dslash_launch_cand(int cand, const DslashArgs<LF, NR, FIN> &a, int nsites, cudaStream_t s)
+{
+    typedef DsCand<LF, NR, RED> K;
+    switch (cand) {
+    case 1: dslash_kernel<LF, NR, HAS_Y, RED, FIN, K::b1, K::m1><<<(nsites + K::b1 - 1) / K::b1, K::b1, 0, s>>>(a); break;
+    case 2: dslash_kernel<LF, NR, HAS_Y, RED, FIN, K::b2, K::m2><<<(nsites + K::b2 - 1) / K::b2, K::b2, 0, s>>>(a); break;
+    default: dslash_kernel<LF, NR, HAS_Y, RED, FIN, K::b0, K::m0><<<(nsites + K::b0 - 1) / K::b0, K::b0, 0, s>>>(a); break;
+    }
+}
+
+template <class LF, int NR, bool HAS_Y, bool RED>
+inline std::string dslash_tune_name()
+{
+    return std::string("dslash ") + LF::name + " nr=" + std::to_string(NR) + " y=" + std::to_string((int)HAS_Y) +
+           " red=" + std::to_string((int)RED);
+}
+
+// Times the three candidates of an instantiation on scratch spinors (the caller's links) with
+// CUDA events on stream s and records the fastest; returns its index (0 when timing fails).
+template <class LF, int NR, bool HAS_Y, bool RED>
+int dslash_tune(const Geom &g, const LF &links, cudaStream_t s, const std::string &key)
+{
+    typedef typename LF::real R;
+    typedef typename LF::store::elem E;
+    const size_t vec = (size_t)LF::store::planes * g.Vh;
+    void *in = nullptr, *out = nullptr, *y = nullptr, *part = nullptr, *tick = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int best = 0;
+    float us[3] = {0, 0, 0};
+    cudaError_t e = cudaMalloc(&in, NR * vec * sizeof(E));
+    if (e == cudaSuccess) e = cudaMalloc(&out, NR * vec * sizeof(E));
+    if (e == cudaSuccess) e = cudaMalloc(&y, NR * vec * sizeof(E));
+    if (e == cudaSuccess) e = cudaMalloc(&part, (size_t)red_chunks(g.Vh) * NR * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&tick, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(in, 0, NR * vec * sizeof(E), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(y, 0, NR * vec * sizeof(E), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(tick, 0, sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) {
+        DslashArgs<LF, NR, NoFin> t;
+        memset(&t, 0, sizeof(t));
+        t.g = g;
+        t.p_out = 1;
+        t.links = links;
+        t.in = (const E *)in;
+        t.out = (E *)out;
+        t.y = HAS_Y ? (const E *)y : nullptr;
+        t.stride = vec;
+        t.alpha = (R)0.01;
+        t.beta = (R)-0.5;
+        t.partials = (double *)part;
+        t.ticket = (unsigned *)tick;
+        for (int cand = 0; cand < 3 && e == cudaSuccess; cand++) {
+            dslash_launch_cand<LF, NR, HAS_Y, RED, NoFin>(cand, t, g.Vh, s);  // warm-up
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < 4; r++) dslash_launch_cand<LF, NR, HAS_Y, RED, NoFin>(cand, t, g.Vh, s);
+            cudaEventRecord(e1, s);
+            e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            us[cand] = ms * 1e3f / 4.f;
+        }
+        if (e == cudaSuccess) {
+            for (int cand = 1; cand < 3; cand++)
+                if (us[cand] < us[best]) best = cand;
+            typedef DsCand<LF, NR, RED> K;
+            const DsShape shapes[3] = {{K::b0, K::m0}, {K::b1, K::m1}, {K::b2, K::m2}};
+            tune_put(key, best, us, shapes, 3);
+        }
+    }
+    if (e != cudaSuccess) {
+        best = 0;
+        cudaGetLastError();
+    }
+    for (void *p : {in, out, y, part, tick})
+        if (p) cudaFree(p);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return best;
+}
+
+// The candidate an instantiation runs with: the override, else the tuned choice, tuning it now
+// when it is unknown and the stream is not capturing, else the default.
+template <class LF, int NR, bool HAS_Y, bool RED>
+inline int dslash_candidate(const Geom &g, const LF &links, cudaStream_t s)
+{
+    if (autotune_override() >= 0) return autotune_override();
+    if (!autotune_enabled()) return 0;
+    const std::string key = tune_key(g.Vh, dslash_tune_name<LF, NR, HAS_Y, RED>());
+    const int c = tune_get(key);
+    if (c >= 0) return c;
+    if (stream_capturing(s)) return 0;
+    return dslash_tune<LF, NR, HAS_Y, RED>(g, links, s, key);
+}
+
+// One launch over `nsites` output sites (from a.k_lo) on stream s, in the tuned launch shape
+// (code that captures launches looks the shape up with dslash_candidate before the capture).
+template <class LF, int NR, bool HAS_Y, bool RED, class FIN>
 inline cudaError_t dslash_launch(const DslashArgs<LF, NR, FIN> &a, int nsites, cudaStream_t s)
 {
-    dslash_kernel<LF, NR, HAS_Y, RED, FIN, BLOCK, MINB><<<(nsites + BLOCK - 1) / BLOCK, BLOCK, 0, s>>>(a);
+    dslash_launch_cand<LF, NR, HAS_Y, RED, FIN>(dslash_candidate<LF, NR, HAS_Y, RED>(a.g, a.links, s), a, nsites, s);
     return cudaGetLastError();
 }
 

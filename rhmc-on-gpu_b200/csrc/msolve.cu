@@ -179,8 +179,16 @@ static int ms_phase(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo *
         const void *links, *links64, *r, *p, *h, *s, *ps, *xs, *pt, *tk, *st, *x0, *h64, *t64, *b;
         double alpha[MS_MAX_RHS];
         cudaStream_t stream;
+        int cand[4];  // launch shapes of the captured Dslash instantiations
     } key;
     memset(&key, 0, sizeof(key));
+    // launch shapes (tuned now, outside the capture, when unknown)
+    key.cand[0] = dslash_candidate<LF, NR, false, false>(c->g, lf, s_);
+    key.cand[1] = dslash_candidate<LF, NR, true, true>(c->g, lf, s_);
+    if (ru) {
+        key.cand[2] = dslash_candidate<L64_12, NR, false, false>(c->g, l64, s_);
+        key.cand[3] = dslash_candidate<L64_12, NR, true, false>(c->g, l64, s_);
+    }
     key.kind = 4; key.link_reals = LF::reals; key.link_bytes = (int)sizeof(typename LF::real); key.nr = NR;
     key.chunk = chunk; key.nshift = S; key.vh = Vh; key.ru_every = A.ru_every; key.links = lf.p; key.r = r; key.p = p;
     key.h = h; key.s = s; key.ps = ps; key.xs = xs; key.pt = pt; key.tk = tk; key.st = st; key.stream = s_;
@@ -195,8 +203,8 @@ static int ms_phase(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo *
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
         for (int it = 0; it < chunk; it++) {
-            dslash_launch<LF, NR, false, false, NoFin>(a1, Vh, s_);
-            dslash_launch<LF, NR, true, true, FinAlpha<NR>>(a2, Vh, s_);
+            dslash_launch_cand<LF, NR, false, false, NoFin>(key.cand[0], a1, Vh, s_);
+            dslash_launch_cand<LF, NR, true, true, FinAlpha<NR>>(key.cand[1], a2, Vh, s_);
             ms_resid_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)r, (const E *)s, pt, tk + 2, st);
             ms_update_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)r, (E *)p, st);
         }
@@ -204,8 +212,8 @@ static int ms_phase(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo *
         if (ru) {
             ms_ru_begin_kernel<<<1, 32, 0, s_>>>(st);
             ms_gather_base_kernel<NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, S, stride, xs, (double2 *)x0, st);
-            dslash_launch<L64_12, NR, false, false, NoFin>(u1, Vh, s_);
-            dslash_launch<L64_12, NR, true, false, NoFin>(u2, Vh, s_);
+            dslash_launch_cand<L64_12, NR, false, false, NoFin>(key.cand[2], u1, Vh, s_);
+            dslash_launch_cand<L64_12, NR, true, false, NoFin>(key.cand[3], u2, Vh, s_);
             ms_ru_resid_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, S, stride, (const double2 *)A.b, (const double2 *)t64,
                                                                   (const double2 *)ps, (E *)r, (E *)p, pt, tk + 4, st);
         }

@@ -331,8 +331,13 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
         const void *links, *links64, *xs, *rs, *p, *ap, *h, *h64, *t64, *st, *pt, *tk, *xg, *bg;
         double coef[RB_MAX];
         cudaStream_t stream;
+        int cand[3];  // launch shapes of the captured Dslash instantiations
     } key;
     memset(&key, 0, sizeof(key));
+    // launch shapes (tuned now, outside the capture, when unknown)
+    key.cand[0] = dslash_candidate<L64_18, NR, false, false>(c->g, l64, s_);
+    key.cand[1] = dslash_candidate<LF, NR, false, false>(c->g, lf, s_);
+    key.cand[2] = dslash_candidate<LF, NR, true, true>(c->g, lf, s_);
     key.kind = 2; key.link_reals = LF::reals; key.link_bytes = (int)sizeof(typename LF::real); key.nr = NR;
     key.n_ru = n_ru; key.vh = Vh; key.links = lf.p; key.links64 = l64.p; key.xs = xs; key.rs = rs; key.p = p;
     key.ap = ap; key.h = h; key.h64 = h64; key.t64 = t64; key.st = st; key.pt = pt; key.tk = tk; key.xg = xg;
@@ -345,13 +350,13 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
         rb_accum_kernel<NR, X><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, xg, (X *)xs, st);
-        dslash_launch<L64_18, NR, false, false, NoFin>(d1, Vh, s_);
-        dslash_launch<L64_18, NR, false, false, NoFin>(d2, Vh, s_);
+        dslash_launch_cand<L64_18, NR, false, false, NoFin>(key.cand[0], d1, Vh, s_);
+        dslash_launch_cand<L64_18, NR, false, false, NoFin>(key.cand[0], d2, Vh, s_);
         rb_resid_kernel<NR, S><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, sstride, bg, xg, (const double2 *)t64, (E *)rs, (E *)p,
                                                              co, pt, tk, st);
         for (int it = 0; it < n_ru; it++) {
-            dslash_launch<LF, NR, false, false, NoFin>(s1, Vh, s_);
-            dslash_launch<LF, NR, true, true, FinRBAlpha<NR>>(s2, Vh, s_);
+            dslash_launch_cand<LF, NR, false, false, NoFin>(key.cand[1], s1, Vh, s_);
+            dslash_launch_cand<LF, NR, true, true, FinRBAlpha<NR>>(key.cand[2], s2, Vh, s_);
             rb_xr_kernel<NR, S, X><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, sstride, (X *)xs, (E *)rs, (const E *)p, (const E *)ap, pt,
                                                              tk + 2, st);
             rb_p_kernel<NR, S><<<gv, VEC_BLOCK, 0, s_>>>(Vh, sstride, (const E *)rs, (E *)p, st);

@@ -135,6 +135,7 @@ struct A64S;
 struct L64_18 {
     typedef double real;
     typedef F64S store;
+    static constexpr const char *name = "f64_18";
     static constexpr int planes = 9;
     static constexpr int reals = 18;
     static constexpr int bytes = 144;
@@ -154,12 +155,14 @@ struct L64_18 {
 // FP64 18-real links with spinors in the reference's site-major host layout (A64S)
 struct L64_18A : L64_18 {
     typedef A64S store;
+    static constexpr const char *name = "f64_18_host";
 };
 
 // FP64, 12 reals: 6 double2 planes, row 2 reconstructed
 struct L64_12 {
     typedef double real;
     typedef F64S store;
+    static constexpr const char *name = "f64_12";
     static constexpr int planes = 6;
     static constexpr int reals = 12;
     static constexpr int bytes = 96;
@@ -181,6 +184,7 @@ struct L64_12 {
 struct L32_18 {
     typedef float real;
     typedef F32S store;
+    static constexpr const char *name = "f32_18";
     static constexpr int planes = 5;
     static constexpr int reals = 18;
     static constexpr int bytes = 72;
@@ -204,6 +208,7 @@ struct L32_18 {
 struct L32_12 {
     typedef float real;
     typedef F32S store;
+    static constexpr const char *name = "f32_12";
     static constexpr int planes = 3;
     static constexpr int reals = 12;
     static constexpr int bytes = 48;
@@ -227,6 +232,7 @@ struct L32_12 {
 struct L16_12 {
     typedef float real;
     typedef H16S store;
+    static constexpr const char *name = "f16_12";
     static constexpr int planes = 2;
     static constexpr int reals = 12;
     static constexpr int bytes = 24;

@@ -66,6 +66,41 @@ def _check(rc):
     return rc
 
 
+# ------------------------------------------------------------------ launch-configuration autotuner
+def autotune(enable):
+    """Turns the launch-shape / RHS-packing tuning on or off; returns the previous setting."""
+    return bool(lib().rhmc_autotune(int(bool(enable))))
+
+
+def autotune_override(candidate):
+    """Forces candidate 0..2 for every tuned launch (-1: tuned choices); returns the previous value."""
+    return lib().rhmc_autotune_override(int(candidate))
+
+
+def tune_cache_load(path):
+    _check(lib().rhmc_tune_cache_load(os.fsencode(path)))
+
+
+def tune_cache_save(path=None):
+    _check(lib().rhmc_tune_cache_save(os.fsencode(path) if path else None))
+
+
+def tune_report():
+    """The tuned choices as a dict (the library's JSON table)."""
+    import json
+    L = lib()
+    L.rhmc_tune_report.restype = ctypes.c_long
+    L.rhmc_tune_report.argtypes = [ctypes.c_char_p, ctypes.c_long]
+    n = L.rhmc_tune_report(None, 0)
+    buf = ctypes.create_string_buffer(n)
+    L.rhmc_tune_report(buf, n)
+    return json.loads(buf.value.decode())
+
+
+def tune_clear():
+    _check(lib().rhmc_tune_clear())
+
+
 def _vp(x):
     """Pointer argument: int (device address), numpy array (host), None."""
     if x is None:

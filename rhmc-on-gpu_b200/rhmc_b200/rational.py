@@ -60,11 +60,13 @@ def inverse_power(q, n, eps, optimise=True, grid=3000):
     return 0.0, a, b, err
 
 
-def rational_power(p, n, eps, optimise=True, method="lsq"):
+def rational_power(p, n, eps, optimise=True, method="minimax"):
     """Coefficients of x^p on [eps, 1], p in (-1, 0) or (0, 1), degree n.
-    Returns dict(a0, a, b, min_eps, power, max_rel_err).  method "lsq": the pole-optimised least
-    squares fit above (a0 = 0 for negative powers); "minimax": minimax_power (type (n, n),
-    near-minimax relative error, usually orders of magnitude smaller at the same degree)."""
+    Returns dict(a0, a, b, min_eps, power, max_rel_err).  method "minimax" (default):
+    minimax_power (type (n, n), near-minimax relative error, the kind of approximation the
+    reference's AlgRemez produces, rationalapprox_calc.cc:8-177); "lsq": the pole-optimised least
+    squares fit above (a0 = 0 for negative powers), usually orders of magnitude less accurate at
+    the same degree."""
     if method == "minimax":
         return minimax_power(p, n, eps)
     if method != "lsq":

@@ -33,8 +33,9 @@ def _alternants(e):
 
 @pytest.mark.parametrize("p,n,eps", CASES)
 def test_minimax_beats_least_squares(p, n, eps):
-    mm = R.rational_power(p, n, eps, method="minimax")
-    ls = R.rational_power(p, n, eps)
+    mm = R.rational_power(p, n, eps)  # the default method
+    assert mm.get("method") == "aaa-lawson"
+    ls = R.rational_power(p, n, eps, method="lsq")
     x = np.random.default_rng(7).uniform(np.log(eps), 0.0, 100000)
     x = np.exp(np.sort(x))
     e_mm, e_ls = np.max(np.abs(_err(mm, x))), np.max(np.abs(_err(ls, x)))
