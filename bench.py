@@ -524,7 +524,8 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
         bounds_traj = [(m * m, lmax_t + m * m - NF_ML * NF_ML) for m, _ in species]
         if lmax_t > lmax:
             raise RuntimeError("trajectory start has a larger spectral radius than the approximations cover")
-    for name, mode, fmt in (("fp64", rb.MSOLVE_FP64, rb.LINKS_F64_18), ("mixed", rb.MSOLVE_MIXED, rb.LINKS_F64_12)):
+    for name, mode, fmt in (("fp64", rb.MSOLVE_FP64, rb.LINKS_F64_18), ("mixed", rb.MSOLVE_MIXED, rb.LINKS_F64_12),
+                            ("mixed_f32_schedule", rb.MSOLVE_MIXED, rb.LINKS_F32_12)):
         configure(mode, fmt, 1e-8, no_md=a.nf_steps)
         for s in range(2):
             ctx.select_species(s)
@@ -551,10 +552,12 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
                       "plaquette_proposal": plaq_md, "plaquette_after": ctx.plaquette(),
                       "gpu_launches": ctx.launch_count() - n0}
     traj["speedup_mixed_vs_fp64"] = round(traj["fp64"]["s_per_trajectory"] / traj["mixed"]["s_per_trajectory"], 3)
-    traj["delta_H_abs_diff"] = abs(traj["fp64"]["delta_H"] - traj["mixed"]["delta_H"])
+    traj["speedup_mixed_f32_schedule_vs_fp64"] = round(traj["fp64"]["s_per_trajectory"]
+                                                       / traj["mixed_f32_schedule"]["s_per_trajectory"], 3)
+    traj["delta_H_abs_diff"] = max(abs(traj["fp64"]["delta_H"] - traj[k]["delta_H"]) for k in ("mixed", "mixed_f32_schedule"))
     traj["integrator"] = "leapfrog tau=1, %d steps; md residual 1e-8, metro residual 1e-10 (FP64)" % a.nf_steps
-    traj["plaquette_proposal_abs_diff"] = max(abs(p - q) for p, q in zip(traj["fp64"]["plaquette_proposal"],
-                                                                           traj["mixed"]["plaquette_proposal"]))
+    traj["plaquette_proposal_abs_diff"] = max(abs(p - q) for k in ("mixed", "mixed_f32_schedule")
+                                              for p, q in zip(traj["fp64"]["plaquette_proposal"], traj[k]["plaquette_proposal"]))
     out["trajectory"] = traj
     ctx.close()
     torch.cuda.set_stream(torch.cuda.default_stream(dev))
@@ -606,7 +609,8 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
     have_ms = False
     traj = {}
     arms = (("fp64_single_rhs", rb.MSOLVE_FP64, rb.LINKS_F64_18, 1), ("fp64_batched", rb.MSOLVE_FP64, rb.LINKS_F64_18, 0),
-            ("mixed_batched", rb.MSOLVE_MIXED, rb.LINKS_F64_12, 0))
+            ("mixed_batched", rb.MSOLVE_MIXED, rb.LINKS_F64_12, 0),
+            ("mixed_batched_f32_schedule", rb.MSOLVE_MIXED, rb.LINKS_F32_12, 0))
     for name, mode, fmt, single in arms:
         ctx.driver_setup(no_flavours=2, no_ps=nps, no_md=a.b5_steps, integrator=rb.INT_LEAPFROG, residue_metro=1e-10,
                          residue_md=1e-8, metro_mode=mode, metro_fmt=fmt, md_mode=mode, md_fmt=fmt, single_rhs=single)
@@ -633,7 +637,7 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
                       "plaquette_after": ctx.plaquette(), "gpu_launches": ctx.launch_count() - n0,
                       "device_memory_in_use_gb": round((total - free) / 1e9, 2)}
         print("rhmc48: %s trajectory %.1f s, dH %.6g" % (name, dt, dS), file=sys.stderr, flush=True)
-    for k in ("fp64_batched", "mixed_batched"):
+    for k in ("fp64_batched", "mixed_batched", "mixed_batched_f32_schedule"):
         traj["speedup_%s_vs_fp64_single_rhs" % k] = round(traj["fp64_single_rhs"]["s_per_trajectory"]
                                                           / traj[k]["s_per_trajectory"], 3)
     traj["delta_H_abs_diff_max"] = max(abs(traj[k]["delta_H"] - traj["fp64_single_rhs"]["delta_H"]) for k, *_ in arms)

@@ -112,6 +112,11 @@ int rhmc_dslash_repeat(rhmc_ctx *ctx, int fmt, void *even, void *odd, int n, int
  * t-slabs that the Dslash consumes as they arrive; a page-locked `out` is written by the kernel
  * directly, any other `out` through a copy per chunk. */
 int rhmc_dslash_host(rhmc_ctx *ctx, int parity_out, double *out, const double *in);
+/* No counterpart in the reference.  The half-Dslash onto the output sites [k_lo, k_lo + k_count) of
+ * parity parity_out only, FP64 18-real links, device spinors in the reference's site-major layout
+ * (complex[Vh][3]); the other output sites are not written.  For domain decomposition: a rank's
+ * context holds its t-slab extended by one ghost slice each side, and this computes its interior. */
+int rhmc_dslash_sites(rhmc_ctx *ctx, int parity_out, double *out, const double *in, long k_lo, long k_count);
 /* out = (M^dag M + shift) in on even sites = (mass^2 + shift) in - Deo Doe in
  * (lib/Action/Inverter/inverter.cc:3, 206-216); internal-layout device spinors. */
 int rhmc_mdagm(rhmc_ctx *ctx, int fmt, void *out, const void *in, double shift, int n);

@@ -290,6 +290,16 @@ static void *mapped_host(void *p, size_t bytes)
 
 extern "C" {
 
+int rhmc_dslash_sites(rhmc_ctx *c, int parity_out, double *out, const double *in, long k_lo, long k_count)
+{
+    if (!c || !out || !in || (parity_out != 0 && parity_out != 1)) return fail(RHMC_ERR_ARG, "bad argument");
+    if (k_lo < 0 || k_count < 1 || k_lo + k_count > c->Vh)
+        return fail(RHMC_ERR_ARG, "rhmc_dslash_sites: sites [%ld, %ld) outside [0, %ld)", k_lo, k_lo + k_count, c->Vh);
+    cudaError_t e = launch_dslash_f64_range(c, c->stream, parity_out, out, in, (int)k_lo, (int)k_count);
+    if (e != cudaSuccess) return cuda_fail(e, "rhmc_dslash_sites");
+    return RHMC_OK;
+}
+
 int rhmc_dslash_host(rhmc_ctx *c, int parity_out, double *out, const double *in)
 {
     if (!c || !out || !in || (parity_out != 0 && parity_out != 1)) return fail(RHMC_ERR_ARG, "bad argument");

@@ -230,6 +230,11 @@ class Context:
     def dslash_host(self, parity_out, out, inp):
         self.call("rhmc_dslash_host", parity_out, out, inp)
 
+    def dslash_sites(self, parity_out, out, inp, k_lo, k_count):
+        """Half-Dslash onto output sites [k_lo, k_lo + k_count) only; out, inp: device arrays in
+        the reference layout (complex (Vh, 3)), e.g. torch complex128 CUDA tensors."""
+        self.call("rhmc_dslash_sites", parity_out, out, inp, ctypes.c_long(k_lo), ctypes.c_long(k_count))
+
     def mdagm(self, fmt, out, inp, shift=0.0, n=1):
         self.call("rhmc_mdagm", fmt, out, inp, float(shift), n)
 

@@ -68,7 +68,16 @@ def rational_power(p, n, eps, optimise=True, method="minimax"):
     squares fit above (a0 = 0 for negative powers), usually orders of magnitude less accurate at
     the same degree."""
     if method == "minimax":
-        return minimax_power(p, n, eps)
+        try:
+            return minimax_power(p, n, eps)
+        except ValueError as e:
+            if not (0.0 < abs(p) < 1.0):
+                raise
+            # AAA finds spurious pole pairs when n is far more than the power needs (x^(1/32)
+            # with 20 poles); the least-squares fit keeps n real negative poles there
+            out = rational_power(p, n, eps, optimise, method="lsq")
+            out["method"] = "lsq (minimax: %s)" % e
+            return out
     if method != "lsq":
         raise ValueError("method must be 'lsq' or 'minimax'")
     if 0.0 < -p < 1.0:
