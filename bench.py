@@ -39,6 +39,16 @@ SPINOR_BYTES = {0: 48, 1: 48, 2: 24, 3: 24, 4: 16}  # 4: half with a per-site sc
 FLOPS_PER_SITE = 570
 
 
+def approx_report(groups):
+    """Each approximation's degree, method and maximum relative error on its interval (what the
+    reference prints for every approximation it builds, lib/Tools/RationalApprox/
+    rationalapprox_calc.cc:42): groups = one [first, md, last] list per species."""
+    roles = ("first (heatbath)", "md (force)", "last (action)")
+    return [{"species": si, "role": roles[j], "power": c["power"], "poles": len(c["b"]),
+             "method": c.get("method", "lsq"), "max_rel_err": c["max_rel_err"]}
+            for si, g in enumerate(groups) for j, c in enumerate(g)]
+
+
 def half_dslash_bytes(fmt, Vh, nrhs=1):
     return Vh * (8 * LINK_BYTES[fmt] + 2 * SPINOR_BYTES[fmt] * nrhs)
 
@@ -395,7 +405,8 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
                       "degree": NF_DEG, "eig_bounds": bounds, "start": "Haar (hot) for kernels and finite differences; "
                       + ("Haar" if a.nf_start == "haar" else "exp(i 0.3 H) of a Gaussian algebra element H per link")
                       + " for the trajectories",
-                      "approx_max_rel_err": max(c["max_rel_err"] for ap_ in approx for c in ap_)}}
+                      "approx_max_rel_err": max(c["max_rel_err"] for ap_ in approx for c in ap_),
+                      "approximations": approx_report(approx)}}
 
     def configure(md_mode, md_fmt, residue_md, no_md=20):
         ctx.driver_setup(no_flavours=2, no_ps=1, no_md=no_md, integrator=rb.INT_LEAPFROG, residue_metro=1e-10,
@@ -605,7 +616,8 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
                       "start": "exp(i 0.3 H) of a Gaussian algebra element H per link",
                       "integrator": "leapfrog tau=1, %d steps; force solves 1e-8, heatbath/action solves 1e-10"
                                     % a.b5_steps,
-                      "approx_max_rel_err": max(c["max_rel_err"] for ap_ in approx for c in ap_)}}
+                      "approx_max_rel_err": max(c["max_rel_err"] for ap_ in approx for c in ap_),
+                      "approximations": approx_report(approx)}}
     have_ms = False
     traj = {}
     arms = (("fp64_single_rhs", rb.MSOLVE_FP64, rb.LINKS_F64_18, 1), ("fp64_batched", rb.MSOLVE_FP64, rb.LINKS_F64_18, 0),
@@ -687,7 +699,8 @@ def rhmc4_bench(a, rb, F, np, torch, rank, dev, stream):
     ctx.close()
     out = {"config": {"lattice": list(dims), "no_flavours": 2, "mass": 0.1, "beta": 5.5, "degree": 8, "range": [lo, 64.0],
                       "integrator": "leapfrog tau=1, 10 steps", "residual": 1e-10, "trajectories": ntraj,
-                      "approx_max_rel_err": max(c["max_rel_err"] for c in ap_)},
+                      "approx_max_rel_err": max(c["max_rel_err"] for c in ap_),
+                      "approximations": approx_report([ap_])},
            "b200": gpu, "b200_s_per_trajectory": round(float(np.median(t_gpu)), 5)}
     try:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

@@ -5,8 +5,9 @@
 // warm-ups, and prints registers, spills, resident blocks and GB/s of algorithmic traffic.
 // DslashCfg encodes the fastest pair of each case.  Inputs are deterministic patterns (the
 // timing does not depend on the values).
-//   make -C rhmc-on-gpu_b200 tune && rhmc-on-gpu_b200/_build/dslash_tune 32 32 [filter]
-// filter: run only the cases whose "<format> NR=<n> red=<0|1>" label contains it.
+//   make -C rhmc-on-gpu_b200 tune && rhmc-on-gpu_b200/_build/dslash_tune 32 32 [filter [shape]]
+// filter: run only the cases whose "<format> NR=<n> red=<0|1>" label contains it; shape
+// "<block>x<minb>": run only that launch shape (for a profiler capture).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -23,37 +24,49 @@ static void *Ubuf, *In, *Out, *Y, *Part;
 static unsigned *Tick;
 static cudaEvent_t e0, e1;
 static const char *Filter = nullptr;
+static const char *Only = nullptr;  // "<block>x<minb>": run only that launch shape
 
-template <class LF, int NR, bool RED, int B, int MB>
+// RED: the solver's D_eo launch (y read, fused reduction); YONLY: y read without the reduction
+template <class LF, int NR, bool RED, int B, int MB, bool YONLY = false>
 void timeit(const char *lname, LF lf)
 {
     typedef typename LF::real R;
     typedef typename LF::store::elem E;
+    if (Only) {
+        char shape[32];
+        snprintf(shape, sizeof(shape), "%dx%d", B, MB);
+        if (strcmp(shape, Only)) return;
+    }
     DslashArgs<LF, NR, NoFin> a;
     memset(&a, 0, sizeof(a));
-    a.g = G; a.p_out = 1; a.links = lf; a.in = (const E *)In; a.out = (E *)Out; a.y = RED ? (const E *)Y : nullptr;
+    a.g = G; a.p_out = 1; a.links = lf; a.in = (const E *)In; a.out = (E *)Out; a.y = (RED || YONLY) ? (const E *)Y : nullptr;
     a.stride = (size_t)LF::store::planes * G.Vh; a.alpha = (R)0.01; a.beta = (R)-0.5; a.use_alphas = 0;
     for (int r = 0; r < NR; r++) a.alphas[r] = (R)0.01;
     a.partials = (double *)Part; a.ticket = Tick;
-    auto kern = dslash_kernel<LF, NR, RED, RED, NoFin, B, MB>;
+    auto kern = dslash_kernel<LF, NR, RED || YONLY, RED, NoFin, B, MB>;
+    const int grid = (int)(((long)G.Vh + B - 1) / B);
     cudaFuncAttributes fa;
     cudaFuncGetAttributes(&fa, kern);
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, B, 0);
-    for (int i = 0; i < 3; i++) CKE((dslash_launch<LF, NR, RED, RED, NoFin, B, MB>(a, G.Vh, 0)));
+    for (int i = 0; i < 3; i++) {
+        kern<<<grid, B>>>(a);
+        CKE(cudaGetLastError());
+    }
     CKE(cudaDeviceSynchronize());
     const int REP = 20;
     cudaEventRecord(e0);
-    for (int i = 0; i < REP; i++) dslash_launch<LF, NR, RED, RED, NoFin, B, MB>(a, G.Vh, 0);
+    for (int i = 0; i < REP; i++) kern<<<grid, B>>>(a);
     cudaEventRecord(e1);
     CKE(cudaEventSynchronize(e1));
     float ms;
     cudaEventElapsedTime(&ms, e0, e1);
     ms /= REP;
     const double ws = LF::store::planes == 1 ? 16.0 / 6.0 : sizeof(typename LF::store::real);  // bytes per spinor real
-    const double bytes = (double)G.Vh * (8.0 * LF::bytes + NR * (12.0 + (RED ? 6.0 : 0.0)) * ws);
-    printf("%-7s NR=%d red=%d block=%3d minb=%d regs=%3d spill=%4d blocks/SM=%d  %8.1f us  %7.1f GB/s\n", lname, NR,
-           (int)RED, B, MB, fa.numRegs, (int)fa.localSizeBytes, nb, ms * 1e3, bytes / (ms * 1e-3) / 1e9);
+    const double bytes = (double)G.Vh * (8.0 * LF::bytes + NR * (12.0 + ((RED || YONLY) ? 6.0 : 0.0)) * ws);
+    printf("%-7s NR=%d red=%d y=%d block=%3d minb=%d regs=%3d spill=%4d blocks/SM=%d  %8.1f us  %7.1f GB/s\n", lname,
+           NR, (int)RED, (int)(RED || YONLY), B, MB, fa.numRegs, (int)fa.localSizeBytes, nb, ms * 1e3,
+           bytes / (ms * 1e-3) / 1e9);
 }
 
 template <class LF, int NR, bool RED>
@@ -69,12 +82,19 @@ void sweep(const char *n, LF lf)
     timeit<LF, NR, RED, 128, 4>(n, lf);
     timeit<LF, NR, RED, 128, 6>(n, lf);
     if constexpr (!RED) timeit<LF, NR, RED, 64, 8>(n, lf);  // the reductions need blocks of 128 or 256 threads
+    // the y read alone, to separate its cost from the reduction's
+    if constexpr (RED) {
+        timeit<LF, NR, false, 128, 3, true>(n, lf);
+        timeit<LF, NR, false, 128, 4, true>(n, lf);
+        timeit<LF, NR, false, 256, 2, true>(n, lf);
+    }
 }
 
 int main(int argc, char **argv)
 {
     const int nx = argc > 1 ? atoi(argv[1]) : 32, nt = argc > 2 ? atoi(argv[2]) : 32;
     Filter = argc > 3 ? argv[3] : nullptr;
+    Only = argc > 4 ? argv[4] : nullptr;
     G = Geom{nx, nx, nx, nt, nx * nx * nx * nt / 2, 1};
     const long Vh = G.Vh;
     printf("lattice %d^3x%d Vh=%ld\n", nx, nt, Vh);
