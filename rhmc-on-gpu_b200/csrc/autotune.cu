@@ -190,6 +190,33 @@ bool stream_capturing(cudaStream_t s)
     return st != cudaStreamCaptureStatusNone;
 }
 
+int persistent_grid(const void *kern, int block, int ntiles)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, std::pair<const void *, int>>, int> waves;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return ntiles;
+    const auto key = std::make_pair(dev, std::make_pair(kern, block));
+    int wave;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = waves.find(key);
+        if (it != waves.end()) {
+            wave = it->second;
+        } else {
+            int nsm = 0, nb = 0;
+            if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, block, 0) == cudaSuccess)
+                wave = nsm * nb;
+            else
+                wave = 0;
+            cudaGetLastError();
+            waves[key] = wave;
+        }
+    }
+    return (wave > 0 && ntiles > wave) ? wave : ntiles;
+}
+
 }  // namespace rhmc
 
 using namespace rhmc;

@@ -36,5 +36,9 @@ void tune_put(const std::string &key, int choice, const float *us, const DsShape
 std::string tune_key(long vh, const std::string &what);
 // true when stream s is capturing (nothing may be timed on it then)
 bool stream_capturing(cudaStream_t s);
+// Grid for a kernel that walks ntiles tiles of `block` threads with stride gridDim.x: one wave of
+// persistent blocks (SMs x resident blocks of that kernel on the current device, queried once
+// per device and kernel), or ntiles when that is smaller or unknown.
+int persistent_grid(const void *kern, int block, int ntiles);
 
 }  // namespace rhmc

@@ -205,7 +205,8 @@ static int ms_phase(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo *
         for (int it = 0; it < chunk; it++) {
             dslash_launch_cand<LF, NR, false, false, NoFin>(key.cand[0], a1, Vh, s_);
             dslash_launch_cand<LF, NR, true, true, FinAlpha<NR>>(key.cand[1], a2, Vh, s_);
-            ms_resid_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (E *)r, (const E *)s, pt, tk + 2, st);
+            ms_resid_kernel<Rv, NR><<<persistent_grid((const void *)ms_resid_kernel<Rv, NR>, VEC_BLOCK, gv), VEC_BLOCK, 0,
+                                      s_>>>(Vh, stride, (E *)r, (const E *)s, pt, tk + 2, st);
             ms_update_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)r, (E *)p, st);
         }
         ms_flush_kernel<Rv, double, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, S, stride, (const E *)r, (double2 *)ps, xs, pt, tk + 3, st);

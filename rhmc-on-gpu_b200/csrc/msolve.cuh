@@ -289,29 +289,41 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_resid_kernel(int Vh, size_t stri
     const int wp = *(volatile const int *)&st->wpos;
     const E *rprev = ring + (size_t)((wp + MS_WIN - 1) % MS_WIN) * NR * stride;
     E *r = ring + (size_t)wp * NR * stride;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    double red[NR];
+    int run[NR];
+    Rv om[NR];
 #pragma unroll
-    for (int j = 0; j < NR; j++) red[j] = 0.0;
-    if (k < Vh) {
+    for (int j = 0; j < NR; j++) {
+        run[j] = st->rhs[j].running;
+        om[j] = (Rv)st->rhs[j].omega;
+    }
+    // tiles of VEC_BLOCK sites walked by a persistent grid (persistent_grid), so the reduction's
+    // per-block fence and ticket are paid once per block
+    const int ntiles = (Vh + VEC_BLOCK - 1) / VEC_BLOCK;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int k = tile * VEC_BLOCK + threadIdx.x;
+        double red[NR];
 #pragma unroll
-        for (int j = 0; j < NR; j++) {
-            if (!st->rhs[j].running) continue;
-            const Rv om = (Rv)st->rhs[j].omega;
+        for (int j = 0; j < NR; j++) red[j] = 0.0;
+        if (k < Vh) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const size_t o = j * stride + (size_t)c * Vh + k;
-                E rv = rprev[o];
-                const E sv = s[o];
-                rv.x = rv.x + om * sv.x;
-                rv.y = rv.y + om * sv.y;
-                r[o] = rv;
-                red[j] += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+            for (int j = 0; j < NR; j++) {
+                if (!run[j]) continue;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const size_t o = j * stride + (size_t)c * Vh + k;
+                    E rv = rprev[o];
+                    const E sv = s[o];
+                    rv.x = rv.x + om[j] * sv.x;
+                    rv.y = rv.y + om[j] * sv.y;
+                    r[o] = rv;
+                    red[j] += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+                }
             }
         }
+        reduce_tile<NR>(red, partials, tile);
     }
     FinLambda<NR> fin{st};
-    reduce_finalize<NR>(red, partials, ticket, fin);
+    reduce_last<NR>(partials, ticket, ntiles * (VEC_BLOCK / RED_CHUNK), fin);
 }
 
 // p = r_m + gamma p (the base search direction; the shifted p_i and x_i are updated once per

@@ -202,33 +202,39 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride,
 {
     typedef typename S::real Rs;
     if (*(volatile const int *)&st->stop) return;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    double red[NR];
+    // tiles of VEC_BLOCK sites walked by a persistent grid (persistent_grid)
+    const int ntiles = (Vh + VEC_BLOCK - 1) / VEC_BLOCK;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int k = tile * VEC_BLOCK + threadIdx.x;
+        double red[NR];
 #pragma unroll
-    for (int j = 0; j < NR; j++) red[j] = 0.0;
-    if (k < Vh) {
+        for (int j = 0; j < NR; j++) red[j] = 0.0;
+        if (k < Vh) {
 #pragma unroll
-        for (int j = 0; j < NR; j++) {
-            if (st->conv[j] || st->hold[j]) continue;
-            const Rs a = (Rs)st->alpha[j];
-            const vec3<Rs> pv = S::template load<Rs>(p + j * sstride, Vh, k), av = S::template load<Rs>(ap + j * sstride, Vh, k);
-            vec3<Rs> rv = S::template load<Rs>(rs + j * sstride, Vh, k);
+            for (int j = 0; j < NR; j++) {
+                if (st->conv[j] || st->hold[j]) continue;
+                const Rs a = (Rs)st->alpha[j];
+                const vec3<Rs> pv = S::template load<Rs>(p + j * sstride, Vh, k),
+                               av = S::template load<Rs>(ap + j * sstride, Vh, k);
+                vec3<Rs> rv = S::template load<Rs>(rs + j * sstride, Vh, k);
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const size_t o = j * stride + (size_t)c * Vh + k;
-                X xv = xs[o];
-                xv.x += a * pv.c[c].re;
-                xv.y += a * pv.c[c].im;
-                xs[o] = xv;
-                rv.c[c].re -= a * av.c[c].re;
-                rv.c[c].im -= a * av.c[c].im;
-                red[j] += (double)rv.c[c].re * rv.c[c].re + (double)rv.c[c].im * rv.c[c].im;
+                for (int c = 0; c < 3; c++) {
+                    const size_t o = j * stride + (size_t)c * Vh + k;
+                    X xv = xs[o];
+                    xv.x += a * pv.c[c].re;
+                    xv.y += a * pv.c[c].im;
+                    xs[o] = xv;
+                    rv.c[c].re -= a * av.c[c].re;
+                    rv.c[c].im -= a * av.c[c].im;
+                    red[j] += (double)rv.c[c].re * rv.c[c].re + (double)rv.c[c].im * rv.c[c].im;
+                }
+                S::template store<Rs>(rs + j * sstride, Vh, k, rv);
             }
-            S::template store<Rs>(rs + j * sstride, Vh, k, rv);
         }
+        reduce_tile<NR>(red, partials, tile);
     }
     FinRBBeta<NR> fin{st};
-    reduce_finalize<NR>(red, partials, ticket, fin);
+    reduce_last<NR>(partials, ticket, ntiles * (VEC_BLOCK / RED_CHUNK), fin);
 }
 
 // p = rs + beta p
@@ -357,8 +363,8 @@ static int rb_group(rhmc_ctx *c, const LF &lf, const double *coef, const double 
         for (int it = 0; it < n_ru; it++) {
             dslash_launch_cand<LF, NR, false, false, NoFin>(key.cand[1], s1, Vh, s_);
             dslash_launch_cand<LF, NR, true, true, FinRBAlpha<NR>>(key.cand[2], s2, Vh, s_);
-            rb_xr_kernel<NR, S, X><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, sstride, (X *)xs, (E *)rs, (const E *)p, (const E *)ap, pt,
-                                                             tk + 2, st);
+            rb_xr_kernel<NR, S, X><<<persistent_grid((const void *)rb_xr_kernel<NR, S, X>, VEC_BLOCK, gv), VEC_BLOCK, 0,
+                                     s_>>>(Vh, stride, sstride, (X *)xs, (E *)rs, (const E *)p, (const E *)ap, pt, tk + 2, st);
             rb_p_kernel<NR, S><<<gv, VEC_BLOCK, 0, s_>>>(Vh, sstride, (const E *)rs, (E *)p, st);
         }
         ce = cudaStreamEndCapture(s_, &graph);

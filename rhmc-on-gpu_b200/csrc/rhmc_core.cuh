@@ -528,13 +528,16 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double *smem)
 // Sites are summed in fixed chunks of RED_CHUNK = 128 consecutive threads: every thread parks
 // its N values in shared memory; value j of a chunk is reduced by one warp, lane l adding
 // threads l, l+32, l+64, l+96 in that order before a shuffle tree (one shuffle tree per value
-// and chunk instead of one per value and warp).  Every block writes one partial per chunk it
-// covers (blockDim must be 128 or 256); the last block to finish (atomic ticket) sums the chunk
-// partials with its first 128 threads (thread t takes chunks t, t+128, ... in order), then a
-// shuffle tree per warp and the 4 warp sums in order, re-arms the ticket and hands the totals to
-// fin(), which every thread of that block calls (a finaliser may split its work across them).  A batched launch (NR right-hand sides, 128-thread blocks) therefore
-// reduces each RHS bit for bit as a single-RHS launch (256-thread blocks) does.
-// All threads of every block must call it.  partials: red_chunks(n) * N doubles.
+// and chunk instead of one per value and warp).  Every tile of blockDim threads (blockDim 128 or
+// 256) writes one partial per chunk it covers (reduce_tile); after its last tile each block takes
+// a ticket, and the last block to finish sums the chunk partials with its first 128 threads
+// (thread t takes chunks t, t+128, ... in order), then a shuffle tree per warp and the 4 warp
+// sums in order, re-arms the ticket and hands the totals to fin(), which every thread of that
+// block calls (a finaliser may split its work across them) (reduce_last).  Neither the block
+// size nor the number of tiles a block walks changes a sum, so a batched launch (NR right-hand
+// sides, 128-thread blocks) reduces each RHS bit for bit as a single-RHS launch (256-thread
+// blocks) does, and a persistent grid as one block per tile does.  All threads of every block
+// must call both parts.  partials: red_chunks(n) * N doubles.
 struct NoFin {
     __device__ void operator()(const double *) const {}
 };
@@ -545,11 +548,13 @@ constexpr int RED_BLOCK_MAX = 256;
 // number of chunk partials a reduction over n threads may write, for blocks of 128 or 256
 __host__ __device__ __forceinline__ long red_chunks(long n) { return 2 * ((n + 255) / 256); }
 
-template <int N, class FIN>
-__device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials, unsigned *ticket, const FIN &fin)
+// Part 1, once per tile of blockDim.x threads (tile = blockIdx.x for one tile per block; a
+// persistent block calls it for each of its tiles): the chunk partials of the tile.  Ends with a
+// barrier, so the caller may reuse shared memory afterwards.
+template <int N>
+__device__ __forceinline__ void reduce_tile(double (&v)[N], double *partials, int tile)
 {
     __shared__ double sm[N][RED_BLOCK_MAX];
-    __shared__ int am_last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int cpb = blockDim.x / RED_CHUNK;
 #pragma unroll
@@ -563,19 +568,30 @@ __device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials
             t += sm[j][base + lane + 64];
             t += sm[j][base + lane + 96];
             t = warp_sum(t);
-            if (lane == 0) partials[((size_t)blockIdx.x * cpb + c) * N + j] = t;
+            if (lane == 0) partials[((size_t)tile * cpb + c) * N + j] = t;
         }
-        if (lane == 0 && wl < N) __threadfence();
     }
     __syncthreads();
+}
+
+// Part 2, once per block after its last tile: the last block to arrive (atomic ticket) sums the
+// nch chunk partials and calls fin().  The block's partials were ordered before this by the
+// barrier that ends reduce_tile; thread 0's fence makes them visible before its ticket.
+template <int N, class FIN>
+__device__ __forceinline__ void reduce_last(double *partials, unsigned *ticket, int nch, const FIN &fin)
+{
+    __shared__ int am_last;
+    __shared__ double wsum[N][4];
+    __shared__ double tot[N];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
-        unsigned t = atomicAdd(ticket, 1u);
+        __threadfence();
+        const unsigned t = atomicAdd(ticket, 1u);
         am_last = (t == gridDim.x - 1);
     }
     __syncthreads();
     if (!am_last) return;
     __threadfence();
-    const int nch = (int)gridDim.x * cpb;
     double acc[N];
 #pragma unroll
     for (int j = 0; j < N; j++) acc[j] = 0.0;
@@ -602,22 +618,28 @@ __device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials
     for (int j = 0; j < N; j++) acc[j] = warp_sum(acc[j]);
     if (lane == 0 && wid < 4)
 #pragma unroll
-        for (int j = 0; j < N; j++) sm[j][wid] = acc[j];
+        for (int j = 0; j < N; j++) wsum[j][wid] = acc[j];
     __syncthreads();
-    __shared__ double tot[N];
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int j = 0; j < N; j++) {
-            double t = sm[j][0];
-            t += sm[j][1];
-            t += sm[j][2];
-            t += sm[j][3];
+            double t = wsum[j][0];
+            t += wsum[j][1];
+            t += wsum[j][2];
+            t += wsum[j][3];
             tot[j] = t;
         }
         *ticket = 0;
     }
     __syncthreads();
     fin(tot);
+}
+
+template <int N, class FIN>
+__device__ __forceinline__ void reduce_finalize(double (&v)[N], double *partials, unsigned *ticket, const FIN &fin)
+{
+    reduce_tile<N>(v, partials, blockIdx.x);
+    reduce_last<N>(partials, ticket, (int)gridDim.x * (int)(blockDim.x / RED_CHUNK), fin);
 }
 
 }  // namespace rhmc

@@ -5,9 +5,11 @@
 // warm-ups, and prints registers, spills, resident blocks and GB/s of algorithmic traffic.
 // DslashCfg encodes the fastest pair of each case.  Inputs are deterministic patterns (the
 // timing does not depend on the values).
-//   make -C rhmc-on-gpu_b200 tune && rhmc-on-gpu_b200/_build/dslash_tune 32 32 [filter [shape]]
+//   make -C rhmc-on-gpu_b200 tune && rhmc-on-gpu_b200/_build/dslash_tune 32 32 [filter [shape [persist]]]
 // filter: run only the cases whose "<format> NR=<n> red=<0|1>" label contains it; shape
-// "<block>x<minb>": run only that launch shape (for a profiler capture).
+// "<block>x<minb>": run only that launch shape (for a profiler capture; "all": every shape);
+// persist 1: launch one wave of persistent blocks that walk the tiles instead of one block per
+// tile.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -25,6 +27,8 @@ static unsigned *Tick;
 static cudaEvent_t e0, e1;
 static const char *Filter = nullptr;
 static const char *Only = nullptr;  // "<block>x<minb>": run only that launch shape
+static int Persist = 0;             // 1: persistent grid
+static int NSM = 148;
 
 // RED: the solver's D_eo launch (y read, fused reduction); YONLY: y read without the reduction
 template <class LF, int NR, bool RED, int B, int MB, bool YONLY = false>
@@ -44,11 +48,13 @@ void timeit(const char *lname, LF lf)
     for (int r = 0; r < NR; r++) a.alphas[r] = (R)0.01;
     a.partials = (double *)Part; a.ticket = Tick;
     auto kern = dslash_kernel<LF, NR, RED || YONLY, RED, NoFin, B, MB>;
-    const int grid = (int)(((long)G.Vh + B - 1) / B);
+    const int ntiles = (int)(((long)G.Vh + B - 1) / B);
     cudaFuncAttributes fa;
     cudaFuncGetAttributes(&fa, kern);
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, B, 0);
+    // one tile per block, or persistent blocks (one wave: SMs x resident blocks) walking the tiles
+    const int grid = Persist ? (ntiles < NSM * nb ? ntiles : NSM * nb) : ntiles;
     for (int i = 0; i < 3; i++) {
         kern<<<grid, B>>>(a);
         CKE(cudaGetLastError());
@@ -64,8 +70,8 @@ void timeit(const char *lname, LF lf)
     ms /= REP;
     const double ws = LF::store::planes == 1 ? 16.0 / 6.0 : sizeof(typename LF::store::real);  // bytes per spinor real
     const double bytes = (double)G.Vh * (8.0 * LF::bytes + NR * (12.0 + ((RED || YONLY) ? 6.0 : 0.0)) * ws);
-    printf("%-7s NR=%d red=%d y=%d block=%3d minb=%d regs=%3d spill=%4d blocks/SM=%d  %8.1f us  %7.1f GB/s\n", lname,
-           NR, (int)RED, (int)(RED || YONLY), B, MB, fa.numRegs, (int)fa.localSizeBytes, nb, ms * 1e3,
+    printf("%-7s NR=%d red=%d y=%d block=%3d minb=%d grid=%5d regs=%3d spill=%4d blocks/SM=%d  %8.1f us  %7.1f GB/s\n",
+           lname, NR, (int)RED, (int)(RED || YONLY), B, MB, grid, fa.numRegs, (int)fa.localSizeBytes, nb, ms * 1e3,
            bytes / (ms * 1e-3) / 1e9);
 }
 
@@ -94,7 +100,9 @@ int main(int argc, char **argv)
 {
     const int nx = argc > 1 ? atoi(argv[1]) : 32, nt = argc > 2 ? atoi(argv[2]) : 32;
     Filter = argc > 3 ? argv[3] : nullptr;
-    Only = argc > 4 ? argv[4] : nullptr;
+    Only = argc > 4 && strcmp(argv[4], "all") ? argv[4] : nullptr;
+    Persist = argc > 5 ? atoi(argv[5]) : 0;
+    cudaDeviceGetAttribute(&NSM, cudaDevAttrMultiProcessorCount, 0);
     G = Geom{nx, nx, nx, nt, nx * nx * nx * nt / 2, 1};
     const long Vh = G.Vh;
     printf("lattice %d^3x%d Vh=%ld\n", nx, nt, Vh);
