@@ -576,6 +576,7 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
 
 
 B5_ML, B5_MS, B5_BETA, B5_DEG = 0.005, 0.04, 5.8, 20
+B5_POLE_GROUP = 5  # poles per group in the pole-group arm (20 poles: 4 groups)
 
 
 def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
@@ -585,10 +586,13 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
     pole count, so every multi-shift solve runs all 8 together), start exp(i 0.3 H) per link
     (seed 1001), momenta seed 3003, phi seeds 2002/2003, Metropolis uniform seed 4004; synthetic
     data.  One leapfrog trajectory (tau = 1, b5_steps steps; force solves to 1e-8, heatbath and
-    action solves to 1e-10) three times: every solve in plain FP64 (18-real links) one
+    action solves to 1e-10) five times: every solve in plain FP64 (18-real links) one
     pseudofermion at a time (the reference's loop), the same with all right-hand sides batched,
-    and every solve in the mixed batched solver (FP64 12-real multi-shift + FP32 refinement, same
-    targets): seconds per trajectory, Delta H, acceptance, plaquette and device memory in use."""
+    every solve in the mixed batched solver (FP64 12-real multi-shift + FP32 refinement, same
+    targets), the same with the FP32 precision schedule, and the mixed batched solver with the
+    poles taken B5_POLE_GROUP at a time (only one group's shifted solutions on the device):
+    seconds per trajectory, Delta H, acceptance, plaquette, the library's workspace and the
+    device memory in use."""
     from rhmc_b200 import rational as R
     from rhmc_b200 import replicas as RP
     torch.cuda.set_stream(stream)
@@ -620,12 +624,18 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
                       "approximations": approx_report(approx)}}
     have_ms = False
     traj = {}
-    arms = (("fp64_single_rhs", rb.MSOLVE_FP64, rb.LINKS_F64_18, 1), ("fp64_batched", rb.MSOLVE_FP64, rb.LINKS_F64_18, 0),
-            ("mixed_batched", rb.MSOLVE_MIXED, rb.LINKS_F64_12, 0),
-            ("mixed_batched_f32_schedule", rb.MSOLVE_MIXED, rb.LINKS_F32_12, 0))
-    for name, mode, fmt, single in arms:
+    # (name, solver mode, link format, single_rhs, pole_group): pole_group G > 0 solves and uses the
+    # poles G at a time, holding one group's shifted solutions instead of all of them
+    arms = (("fp64_single_rhs", rb.MSOLVE_FP64, rb.LINKS_F64_18, 1, 0),
+            ("fp64_batched", rb.MSOLVE_FP64, rb.LINKS_F64_18, 0, 0),
+            ("mixed_batched", rb.MSOLVE_MIXED, rb.LINKS_F64_12, 0, 0),
+            ("mixed_batched_f32_schedule", rb.MSOLVE_MIXED, rb.LINKS_F32_12, 0, 0),
+            ("mixed_batched_pole_groups_%d" % B5_POLE_GROUP, rb.MSOLVE_MIXED, rb.LINKS_F64_12, 0, B5_POLE_GROUP))
+    for name, mode, fmt, single, pgroup in arms:
+        ctx.workspace_release()  # each arm's workspace high-water mark is its own
         ctx.driver_setup(no_flavours=2, no_ps=nps, no_md=a.b5_steps, integrator=rb.INT_LEAPFROG, residue_metro=1e-10,
-                         residue_md=1e-8, metro_mode=mode, metro_fmt=fmt, md_mode=mode, md_fmt=fmt, single_rhs=single)
+                         residue_md=1e-8, metro_mode=mode, metro_fmt=fmt, md_mode=mode, md_fmt=fmt, single_rhs=single,
+                         pole_group=pgroup)
         if not have_ms:
             ctx.add_species(B5_MS, 1, nps)
             have_ms = True
@@ -647,14 +657,16 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
         free, total = torch.cuda.mem_get_info(dev)
         traj[name] = {"s_per_trajectory": round(dt, 2), "delta_H": dS, "accepted": acc,
                       "plaquette_after": ctx.plaquette(), "gpu_launches": ctx.launch_count() - n0,
+                      "workspace_gb": round(ctx.workspace_bytes() / 1e9, 2),
                       "device_memory_in_use_gb": round((total - free) / 1e9, 2)}
         print("rhmc48: %s trajectory %.1f s, dH %.6g" % (name, dt, dS), file=sys.stderr, flush=True)
-    for k in ("fp64_batched", "mixed_batched", "mixed_batched_f32_schedule"):
+    for k in [n for n, *_ in arms[1:]]:
         traj["speedup_%s_vs_fp64_single_rhs" % k] = round(traj["fp64_single_rhs"]["s_per_trajectory"]
                                                           / traj[k]["s_per_trajectory"], 3)
     traj["delta_H_abs_diff_max"] = max(abs(traj[k]["delta_H"] - traj["fp64_single_rhs"]["delta_H"]) for k, *_ in arms)
-    traj["memory_note"] = ("in use after each arm (library workspaces are kept, so this is the high-water mark "
-                           "of the arms run so far)")
+    traj["memory_note"] = ("workspace_gb: the library's workspaces after the arm (released before it: solver "
+                           "vectors, shifted solutions, driver fields; links, momenta and ipdot come on top); "
+                           "device_memory_in_use_gb: the whole device after the arm")
     out["trajectory"] = traj
     ctx.close()
     torch.cuda.set_stream(torch.cuda.default_stream(dev))

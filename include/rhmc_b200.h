@@ -266,6 +266,15 @@ typedef struct {
     int single_rhs;       /* 1: every pseudofermion of every species in its own multi-shift solve (the
                              reference's loop over pseudofermions, inverter.cc:164); 0: all of them
                              batched into one solve (one link read serves every right-hand side) */
+    int pole_group;       /* 0: all poles of an approximation in one multi-shift solve, every shifted
+                             solution held on the device at once (the reference keeps them all,
+                             smf_device, lib/Cuda/cuda_fermion_force.cu:346-418); G > 0: the poles
+                             in groups of at most G, each group solved, used (its share of the
+                             rational sum, force or action accumulated) and dropped before the
+                             next: the shifted vectors of a solve shrink by order/G at the cost of
+                             repeating the Krylov iterations once per group (no counterpart in
+                             the reference; for volumes or batches whose shifted solutions do not
+                             fit in HBM) */
 } rhmc_driver_params;
 
 /* Configures the driver of lib/Update (update.cc, ipdot.cc, momenta.cc, MD_integrators).
@@ -319,6 +328,15 @@ int rhmc_update(rhmc_ctx *ctx, double uniform, int *acc, double *delta_s);
 int rhmc_save_conf(rhmc_ctx *ctx);
 int rhmc_copy_saved(rhmc_ctx *ctx);
 int rhmc_driver_stats(rhmc_ctx *ctx, long *force_evals, long *solves);
+/* Device memory held by the context's workspaces (solver vectors, shifted solutions, driver
+ * fields, reduction buffers), in bytes; no counterpart in the reference.  Workspaces grow to
+ * the largest request and are kept until rhmc_workspace_release or rhmc_destroy. */
+int rhmc_workspace_bytes(rhmc_ctx *ctx, long *bytes);
+/* Synchronises the context's stream, then frees every workspace and instantiated solver graph
+ * of the context except the state the driver carries between calls (phi, chi and the saved
+ * configuration; links, momenta and ipdot are not workspaces); later calls allocate again what
+ * they need.  No counterpart in the reference. */
+int rhmc_workspace_release(rhmc_ctx *ctx);
 
 /* CUDA-core FMA throughput of this GPU in TFLOP/s (fp64 = 1: FP64, 0: FP32), measured by a
  * microbenchmark (8 independent FMA chains per thread, 8 blocks of 256 threads per SM, CUDA

@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include <random>
@@ -45,7 +46,8 @@ int link_update(rhmc_ctx *c, double step);
 int plaquette_sums(rhmc_ctx *c, double *temporal, double *spatial);
 int momentum_action(rhmc_ctx *c, double *out);
 int rdot(rhmc_ctx *c, const double2 *a, const double2 *b, long n, double *out);
-int rational_sum(rhmc_ctx *c, int nrhs, int nshift, double a0, const double *a, const double2 *x, const double2 *b, double2 *out);
+int rational_sum(rhmc_ctx *c, int nrhs, int nshift, double a0, const double *a, const double2 *x, const double2 *b, double2 *out,
+                 int add);
 
 struct Approx {
     int order = 0;
@@ -159,7 +161,37 @@ struct Solved {
     double2 *x = nullptr;
 };
 
-static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res, int mode, int fmt, Solved &out)
+// Pole groups (rhmc_driver_params.pole_group = G > 0): approximation `which` is applied in
+// ceil(order / G) groups of consecutive poles, each solved, used and dropped before the next, so
+// only one group's shifted solutions (and solver vectors) are on the device at a time; G = 0
+// keeps one group holding every pole.
+static int pole_groups(rhmc_ctx *c, int which)
+{
+    Driver *d = drv(c);
+    const int G = d->P.pole_group;
+    if (G <= 0) return 1;
+    int mx = 0;
+    for (const Species &S : d->sp) mx = std::max(mx, S.approx[which].order);
+    return (mx + G - 1) / G;
+}
+
+// poles [g G, g G + G) of ap (all of them when G == 0); the constant a0 belongs to group 0
+static Approx pole_slice(const Approx &ap, int g, int G)
+{
+    if (G <= 0) return ap;
+    Approx r;
+    const int lo = std::min(g * G, ap.order), hi = std::min(lo + G, ap.order);
+    r.order = hi - lo;
+    r.a0 = g == 0 ? ap.a0 : 0.0;
+    r.min_eps = ap.min_eps;
+    r.a.assign(ap.a.begin() + lo, ap.a.begin() + hi);
+    r.b.assign(ap.b.begin() + lo, ap.b.begin() + hi);
+    return r;
+}
+
+// group g of the poles (species without poles in that group get order 0 and no solve)
+static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res, int mode, int fmt, Solved &out,
+                         int g = 0)
 {
     Driver *d = drv(c);
     const int ns = nspecies(c);
@@ -169,7 +201,7 @@ static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res
     bool same = true;
     size_t xtot = 0;
     for (int s = 0; s < ns; s++) {
-        out.ap.push_back(rescaled(c, s, which));
+        out.ap.push_back(pole_slice(rescaled(c, s, which), g, d->P.pole_group));
         same = same && out.ap[s].order == out.ap[0].order;
         out.xoff.push_back(xtot);
         xtot += (size_t)d->sp[s].no_ps * out.ap[s].order;
@@ -179,6 +211,7 @@ static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res
     if (rc) return rc;
     if (ns == 1 || !same || d->P.single_rhs) {
         for (int s = 0; s < ns; s++) {
+            if (out.ap[s].order == 0) continue;
             double2 *in = nullptr;
             rc = field(c, fname(in_base, s), d->sp[s].no_ps, &in);
             if (rc) return rc;
@@ -270,19 +303,24 @@ static int inv_approx_calc(rhmc_ctx *c, int which, double res)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
-    Solved sv;
-    if ((rc = solve_species(c, which, which == 0 ? "drv_phi" : "drv_chi", res, d->P.metro_mode, d->P.metro_fmt, sv))) return rc;
-    for (int s = 0; s < nspecies(c); s++) {
-        const int nps = d->sp[s].no_ps;
-        const Approx &ap = sv.ap[s];
-        double2 *phi = nullptr, *chi = nullptr;
-        rc = field(c, fname("drv_phi", s), nps, &phi);
-        if (rc) return rc;
-        rc = field(c, fname("drv_chi", s), nps, &chi);
-        if (rc) return rc;
-        const double2 *in = which == 0 ? phi : chi;
-        double2 *out = which == 0 ? chi : phi;
-        if ((rc = rational_sum(c, nps, ap.order, ap.a0, ap.a.data(), sv.x + sv.xoff[s] * SP(c), in, out))) return rc;
+    for (int g = 0; g < pole_groups(c, which); g++) {
+        Solved sv;
+        if ((rc = solve_species(c, which, which == 0 ? "drv_phi" : "drv_chi", res, d->P.metro_mode, d->P.metro_fmt, sv, g)))
+            return rc;
+        for (int s = 0; s < nspecies(c); s++) {
+            const int nps = d->sp[s].no_ps;
+            const Approx &ap = sv.ap[s];
+            if (ap.order == 0) continue;
+            double2 *phi = nullptr, *chi = nullptr;
+            rc = field(c, fname("drv_phi", s), nps, &phi);
+            if (rc) return rc;
+            rc = field(c, fname("drv_chi", s), nps, &chi);
+            if (rc) return rc;
+            const double2 *in = which == 0 ? phi : chi;
+            double2 *out = which == 0 ? chi : phi;
+            // group 0: out = a0 in + its poles; later groups add their poles to out
+            if ((rc = rational_sum(c, nps, ap.order, ap.a0, ap.a.data(), sv.x + sv.xoff[s] * SP(c), in, out, g > 0))) return rc;
+        }
     }
     return RHMC_OK;
 }
@@ -293,12 +331,15 @@ static int fermion_part(rhmc_ctx *c, int add)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
-    Solved sv;
-    if ((rc = solve_species(c, 1, "drv_chi", d->P.residue_md, d->P.md_mode, d->P.md_fmt, sv))) return rc;
-    for (int s = 0; s < nspecies(c); s++) {
-        const Approx &ap = sv.ap[s];
-        rc = fermion_force(c, d->sp[s].no_ps, ap.order, ap.a.data(), sv.x + sv.xoff[s] * SP(c), s == 0 ? add : 1);
-        if (rc) return rc;
+    for (int g = 0; g < pole_groups(c, 1); g++) {
+        Solved sv;
+        if ((rc = solve_species(c, 1, "drv_chi", d->P.residue_md, d->P.md_mode, d->P.md_fmt, sv, g))) return rc;
+        for (int s = 0; s < nspecies(c); s++) {
+            const Approx &ap = sv.ap[s];
+            if (ap.order == 0) continue;
+            rc = fermion_force(c, d->sp[s].no_ps, ap.order, ap.a.data(), sv.x + sv.xoff[s] * SP(c), (g == 0 && s == 0) ? add : 1);
+            if (rc) return rc;
+        }
     }
     d->force_evals++;
     return RHMC_OK;
@@ -312,23 +353,27 @@ static int fermion_action_md(rhmc_ctx *c, double *out)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
-    Solved sv;
-    if ((rc = solve_species(c, 1, "drv_chi", d->P.residue_md, d->P.md_mode, d->P.md_fmt, sv))) return rc;
     double sum = 0.0, v;
-    for (int s = 0; s < nspecies(c); s++) {
-        const int nps = d->sp[s].no_ps;
-        const Approx &ap = sv.ap[s];
-        const double2 *xs = sv.x + sv.xoff[s] * SP(c);
-        double2 *chi = nullptr;
-        rc = field(c, fname("drv_chi", s), nps, &chi);
-        if (rc) return rc;
-        for (int ps = 0; ps < nps; ps++) {
-            const double2 *cp = chi + ps * SP(c);
-            if ((rc = rdot(c, cp, cp, (long)SP(c), &v))) return rc;
-            sum += ap.a0 * v;
-            for (int i = 0; i < ap.order; i++) {
-                if ((rc = rdot(c, cp, xs + ((size_t)ps * ap.order + i) * SP(c), (long)SP(c), &v))) return rc;
-                sum += ap.a[i] * v;
+    for (int g = 0; g < pole_groups(c, 1); g++) {
+        Solved sv;
+        if ((rc = solve_species(c, 1, "drv_chi", d->P.residue_md, d->P.md_mode, d->P.md_fmt, sv, g))) return rc;
+        for (int s = 0; s < nspecies(c); s++) {
+            const int nps = d->sp[s].no_ps;
+            const Approx &ap = sv.ap[s];
+            const double2 *xs = sv.x + sv.xoff[s] * SP(c);
+            double2 *chi = nullptr;
+            rc = field(c, fname("drv_chi", s), nps, &chi);
+            if (rc) return rc;
+            for (int ps = 0; ps < nps; ps++) {
+                const double2 *cp = chi + ps * SP(c);
+                if (g == 0) {
+                    if ((rc = rdot(c, cp, cp, (long)SP(c), &v))) return rc;
+                    sum += ap.a0 * v;
+                }
+                for (int i = 0; i < ap.order; i++) {
+                    if ((rc = rdot(c, cp, xs + ((size_t)ps * ap.order + i) * SP(c), (long)SP(c), &v))) return rc;
+                    sum += ap.a[i] * v;
+                }
             }
         }
     }
@@ -559,6 +604,7 @@ int rhmc_driver_setup(rhmc_ctx *c, const rhmc_driver_params *p)
     if (p->integrator < 0 || p->integrator > RHMC_INT_LEAPFROG) return fail(RHMC_ERR_ARG, "unknown integrator");
     if (p->auto_bounds < 0 || p->auto_bounds > 2) return fail(RHMC_ERR_ARG, "auto_bounds must be 0, 1 or 2");
     if (p->single_rhs != 0 && p->single_rhs != 1) return fail(RHMC_ERR_ARG, "single_rhs must be 0 or 1");
+    if (p->pole_group < 0) return fail(RHMC_ERR_ARG, "pole_group must be 0 (all poles at once) or positive");
     Driver *d = ensure_driver(c);
     d->P = *p;
     d->sp[0].no_flavours = p->no_flavours;
@@ -685,6 +731,35 @@ int rhmc_driver_stats(rhmc_ctx *c, long *force_evals, long *solves)
     if (!c || !c->driver) return fail(RHMC_ERR_STATE, "driver not configured");
     if (force_evals) *force_evals = c->driver->force_evals;
     if (solves) *solves = c->driver->solves;
+    return RHMC_OK;
+}
+
+int rhmc_workspace_bytes(rhmc_ctx *c, long *bytes)
+{
+    if (!c || !bytes) return fail(RHMC_ERR_ARG, "null argument");
+    size_t n = 0;
+    for (const auto &kv : c->ws.buf) n += kv.second.second;
+    *bytes = (long)n;
+    return RHMC_OK;
+}
+
+int rhmc_workspace_release(rhmc_ctx *c)
+{
+    if (!c) return fail(RHMC_ERR_ARG, "null argument");
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "rhmc_workspace_release");
+    c->graphs.release();
+    // keep the buffers that carry state between calls: the pseudofermion fields and the saved
+    // configuration of the Metropolis step
+    for (auto it = c->ws.buf.begin(); it != c->ws.buf.end();) {
+        const std::string &n = it->first;
+        if (n.rfind("drv_phi", 0) == 0 || n.rfind("drv_chi", 0) == 0 || n == "drv_usave") {
+            ++it;
+            continue;
+        }
+        cudaFree(it->second.first);
+        it = c->ws.buf.erase(it);
+    }
     return RHMC_OK;
 }
 

@@ -28,7 +28,8 @@ int gauge_force(rhmc_ctx *c, int mode);
 int fermion_force(rhmc_ctx *c, int nrhs, int nshift, const double *a, const double2 *x, int mode);
 int mom_update(rhmc_ctx *c, double step);
 int link_update(rhmc_ctx *c, double step);
-int rational_sum(rhmc_ctx *c, int nrhs, int nshift, double a0, const double *a, const double2 *x, const double2 *b, double2 *out);
+int rational_sum(rhmc_ctx *c, int nrhs, int nshift, double a0, const double *a, const double2 *x, const double2 *b, double2 *out,
+                 int add);
 int rdot(rhmc_ctx *c, const double2 *a, const double2 *b, long n, double *out);
 
 static rhmc_legacy_config g_cfg;
@@ -485,7 +486,7 @@ void cuda_sol_sum(const int num_shifts, const double mult_const, const double *n
     LEG(stage(c, "leg_stage", 6 * (size_t)c->Vh * nps * 2 * sizeof(float), &d), "cuda_sol_sum");
     for (size_t ps = 0; ps < nps; ps++) {
         LEG(rational_sum(c, 1, num_shifts, mult_const, numerators, g_smf + ps * g_cfg.max_approx_order * n, g_mf + ps * n,
-                         (double2 *)tmp),
+                         (double2 *)tmp, 0),
             "cuda_sol_sum");
         cudaMemcpyAsync(g_mf + ps * n, tmp, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream);
         spinor_to_packed<<<grid_for(c->Vh, 256), 256, 0, c->stream>>>(c->Vh, g_mf + ps * n, 3 * c->V * ps, 3 * c->V * nps,

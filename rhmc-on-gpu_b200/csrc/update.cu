@@ -129,15 +129,21 @@ __global__ void __launch_bounds__(UPD_BLOCK) rdot_kernel(long n, const double2 *
 }
 
 // out[r] = a0 b[r] + sum_i a_i x[r][i]   (all FP64 internal, even)
+// add: out += a0 b + sum_i a_i x_i (a rational sum accumulated over groups of poles)
 __global__ void __launch_bounds__(UPD_BLOCK) rational_sum_kernel(long nel, int nrhs, int nshift, double a0,
                                                                  const double *__restrict__ a, const double2 *__restrict__ x,
-                                                                 const double2 *__restrict__ b, double2 *out)
+                                                                 const double2 *__restrict__ b, double2 *out, int add)
 {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // over nrhs * nel
     if (i >= (long)nrhs * nel) return;
     const long r = i / nel, e = i % nel;
     const double2 bv = b[i];
     double re = a0 * bv.x, im = a0 * bv.y;
+    if (add) {
+        const double2 ov = out[i];
+        re += ov.x;
+        im += ov.y;
+    }
     for (int s = 0; s < nshift; s++) {
         const double2 xv = x[(r * nshift + s) * nel + e];
         re += __ldg(a + s) * xv.x;
@@ -212,14 +218,15 @@ int rdot(rhmc_ctx *c, const double2 *a, const double2 *b, long n, double *out)
     return host_sum(c, (const double *)part, nb, 1, out);
 }
 
-int rational_sum(rhmc_ctx *c, int nrhs, int nshift, double a0, const double *a, const double2 *x, const double2 *b, double2 *out)
+int rational_sum(rhmc_ctx *c, int nrhs, int nshift, double a0, const double *a, const double2 *x, const double2 *b, double2 *out,
+                 int add)
 {
     const long nel = 3 * c->Vh;
     void *da;
     CK(c->ws.get("rs_coef", (size_t)nshift * sizeof(double), &da));
     CK(cudaMemcpyAsync(da, a, nshift * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     rational_sum_kernel<<<grid_for(nrhs * nel, UPD_BLOCK), UPD_BLOCK, 0, c->stream>>>(nel, nrhs, nshift, a0, (const double *)da, x,
-                                                                                      b, out);
+                                                                                      b, out, add);
     c->launches++;
     CK(cudaGetLastError());
     return RHMC_OK;
@@ -281,7 +288,7 @@ int rhmc_rdot(rhmc_ctx *c, const double *a, const double *b, int n, double *out)
 int rhmc_rational_sum(rhmc_ctx *c, int nrhs, int nshift, double a0, const double *a, const double *x, const double *b, double *out)
 {
     if (!c || !a || !x || !b || !out || nrhs < 1 || nshift < 0) return fail(RHMC_ERR_ARG, "bad argument");
-    return rational_sum(c, nrhs, nshift, a0, a, (const double2 *)x, (const double2 *)b, (double2 *)out);
+    return rational_sum(c, nrhs, nshift, a0, a, (const double2 *)x, (const double2 *)b, (double2 *)out, 0);
 }
 
 }  // extern "C"

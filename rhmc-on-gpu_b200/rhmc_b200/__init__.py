@@ -381,14 +381,15 @@ class DriverParams(ctypes.Structure):
                 ("gauge_scale", ctypes.c_int), ("integrator", ctypes.c_int), ("max_cg", ctypes.c_int),
                 ("residue_metro", ctypes.c_double), ("residue_md", ctypes.c_double),
                 ("metro_mode", ctypes.c_int), ("metro_fmt", ctypes.c_int), ("md_mode", ctypes.c_int),
-                ("md_fmt", ctypes.c_int), ("auto_bounds", ctypes.c_int), ("single_rhs", ctypes.c_int)]
+                ("md_fmt", ctypes.c_int), ("auto_bounds", ctypes.c_int), ("single_rhs", ctypes.c_int),
+                ("pole_group", ctypes.c_int)]
 
 
 def _driver_setup(self, no_flavours=2, no_ps=1, no_md=10, gauge_scale=5, integrator=INT_2MN, max_cg=100000,
                   residue_metro=1e-10, residue_md=1e-10, metro_mode=MSOLVE_FP64, metro_fmt=LINKS_F64_18,
-                  md_mode=MSOLVE_FP64, md_fmt=LINKS_F64_18, auto_bounds=0, single_rhs=0):
+                  md_mode=MSOLVE_FP64, md_fmt=LINKS_F64_18, auto_bounds=0, single_rhs=0, pole_group=0):
     p = DriverParams(no_flavours, no_ps, no_md, gauge_scale, integrator, max_cg, residue_metro, residue_md, metro_mode,
-                     metro_fmt, md_mode, md_fmt, auto_bounds, single_rhs)
+                     metro_fmt, md_mode, md_fmt, auto_bounds, single_rhs, pole_group)
     self.no_ps = no_ps
     self.call("rhmc_driver_setup", ctypes.byref(p))
 
@@ -430,6 +431,16 @@ Context.update_nometro = lambda self: self.call("rhmc_update_nometro")
 Context.update = _update
 Context.save_conf = lambda self: self.call("rhmc_save_conf")
 Context.copy_saved = lambda self: self.call("rhmc_copy_saved")
+
+
+def _workspace_bytes(self):
+    n = ctypes.c_long(0)
+    self.call("rhmc_workspace_bytes", ctypes.byref(n))
+    return n.value
+
+
+Context.workspace_bytes = _workspace_bytes
+Context.workspace_release = lambda self: self.call("rhmc_workspace_release")
 
 
 class LegacyConfig(ctypes.Structure):
