@@ -34,8 +34,12 @@ void chiral_meas(complex<REAL> &chiral, complex<REAL> &e_dens, complex<REAL> &b_
 static double h_min = 1.0e-3, h_max = 64.0;
 
 // findminmax (lib/Action/Findminmax/findminmax.cc:140-183) is replaced by fixed bounds so that
-// rescaling (lib/Tools/RationalApprox/rationalapprox.cc:134-266) is deterministic.
+// rescaling (lib/Tools/RationalApprox/rationalapprox.cc:134-266) is deterministic.  The power
+// iterations of that file (findmaxeig, findmineig) are linked in unmodified (the recipe renames
+// only its findminmax) and exposed below.
 void findminmax(REAL &min, REAL &max) { min = h_min; max = h_max; }
+void findmaxeig(REAL &max);
+void findmineig(REAL &min, const REAL &max);
 
 // ------------------------------------------------------------------ friend I/O hooks
 void smartpack_gauge(float out[2 * 12 * no_links], const Conf *in)
@@ -241,6 +245,23 @@ void ref_setup(unsigned long seed)
 }
 
 // make_shift_table (lib/Tools/Packer/packer.cc:415-439) reads the same globals
+// the reference's CPU power iterations for the bounds of M^dag M on the current links
+// (findminmax.cc:12-137): each starts from a Gaussian vector of the reference's own generator and
+// stops when the norm changes by less than 1e-5 relative
+double ref_findmaxeig()
+{
+    REAL mx = 0;
+    findmaxeig(mx);
+    return mx;
+}
+
+double ref_findmineig(double max)
+{
+    REAL mn = 0;
+    findmineig(mn, max);
+    return mn;
+}
+
 void ref_tables(int *table, int *eta_out)
 {
     for (long i = 0; i < size; i++)

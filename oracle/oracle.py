@@ -294,6 +294,9 @@ class RefLib:
         L.ref_read_conf.argtypes = [_D]
         L.ref_trajectory.argtypes = [ctypes.c_int, ctypes.c_double, _I]
         L.ref_trajectory.restype = ctypes.c_double
+        L.ref_findmaxeig.restype = ctypes.c_double
+        L.ref_findmineig.restype = ctypes.c_double
+        L.ref_findmineig.argtypes = [ctypes.c_double]
         L.ref_setup(seed)
 
     # field I/O
@@ -430,6 +433,14 @@ class RefLib:
         a[:n] = approx["a"]
         b[:n] = approx["b"]
         self.lib.ref_set_approx(which, n, approx.get("min_eps", 1e-7), approx["a0"], _dp(a), _dp(b))
+
+    def findmaxeig(self):
+        """lambda_max of M^dag M on the current links by the reference's findmaxeig."""
+        return self.lib.ref_findmaxeig()
+
+    def findmineig(self, mx):
+        """lambda_min of M^dag M by the reference's findmineig (power iteration on mx - M^dag M)."""
+        return self.lib.ref_findmineig(float(mx))
 
     def set_minmax(self, mn, mx):
         self.lib.ref_set_minmax(mn, mx)
