@@ -79,79 +79,148 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
     typedef typename S::elem E;
     // y (read only by the epilogue) is fetched into shared memory by cp.async at the start of a
     // tile, so its DRAM latency overlaps the stencil instead of following it (when it fits)
-    constexpr bool PF = HAS_Y && S::soa && (NR * S::planes * BLOCK * sizeof(E) <= 24576);
+    constexpr bool PF = HAS_Y && S::soa && S::pack == 1 && (NR * S::planes * BLOCK * sizeof(E) <= 24576);
     __shared__ __align__(16) E ysm[PF ? NR * S::planes * BLOCK : 1];
     // tiles of BLOCK consecutive output sites; a launch with fewer blocks than tiles (persistent
     // blocks) walks them with stride gridDim.x, so the per-block work of the fused reduction
     // (fence, ticket) is paid once per block instead of once per tile
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int k = a.k_lo + tile * BLOCK + threadIdx.x;
-        Site s = site_of(a.g, a.p_out, k < kend ? k : a.k_lo);
-        if (PF && k < kend) {
+        if constexpr (S::pack > 1) {
+            // packed right-hand sides: one load brings P of them (PackS)
+            constexpr int P = S::pack, NQ = NR / P;
+            static_assert(NR % P == 0, "the batch is a whole number of packs");
+            typedef PackIO<R, P> IO;
+            double red[NR];
 #pragma unroll
-            for (int r = 0; r < NR; r++)
+            for (int j = 0; j < NR; j++) red[j] = 0.0;
+            if (k < kend) {
+                const Site s = site_of(a.g, a.p_out, k);
+                vec3<R> acc[NR];
 #pragma unroll
-                for (int pl = 0; pl < S::planes; pl++)
-                    cp_async_elem<sizeof(E)>(&ysm[(r * S::planes + pl) * BLOCK + threadIdx.x],
-                                             a.y + r * a.stride + (size_t)pl * Vh + k);
-            cp_async_commit();
-        }
-        double red[NR];
+                for (int r = 0; r < NR; r++)
 #pragma unroll
-        for (int j = 0; j < NR; j++) red[j] = 0.0;
-
-        if (k < kend) {
-            vec3<R> acc[NR];
+                    for (int c = 0; c < 3; c++) acc[r].c[c] = mk<R>(0, 0);
 #pragma unroll
-            for (int r = 0; r < NR; r++)
+                for (int mu = 0; mu < 4; mu++) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) acc[r].c[c] = mk<R>(0, 0);
+                    for (int dir = 0; dir < 2; dir++) {
+                        su3m<R> u;
+                        const int kn = neighbour(a.g, s, mu, dir ? -1 : +1);
+                        if (dir == 0)
+                            a.links.load(mu, a.p_out, k, u, eta_of(a.g, s, mu));
+                        else
+                            a.links.load(mu, 1 - a.p_out, kn, u, eta_back(a.g, s, mu));
 #pragma unroll
-            for (int mu = 0; mu < 4; mu++) {
-                su3m<R> u;
-                const int kf = neighbour(a.g, s, mu, +1);
-                a.links.load(mu, a.p_out, k, u, eta_of(a.g, s, mu));
+                        for (int q = 0; q < NQ; q++) {
+                            vec3<R> v[P];
 #pragma unroll
-                for (int r = 0; r < NR; r++) {
-                    vec3<R> v = LF::store::template load<R>(a.in + r * a.stride, Vh, kf);
-                    mv_acc(u, v, acc[r]);
+                            for (int c = 0; c < 3; c++) {
+                                cpx<R> e[P];
+                                IO::ld(a.in + q * a.stride + (size_t)c * Vh + kn, e);
+#pragma unroll
+                                for (int i = 0; i < P; i++) v[i].c[c] = e[i];
+                            }
+#pragma unroll
+                            for (int i = 0; i < P; i++) {
+                                if (dir == 0)
+                                    mv_acc(u, v[i], acc[q * P + i]);
+                                else
+                                    mdv_sub(u, v[i], acc[q * P + i]);
+                            }
+                        }
+                    }
                 }
-                const int kb = neighbour(a.g, s, mu, -1);
-                a.links.load(mu, 1 - a.p_out, kb, u, eta_back(a.g, s, mu));
 #pragma unroll
-                for (int r = 0; r < NR; r++) {
-                    vec3<R> v = LF::store::template load<R>(a.in + r * a.stride, Vh, kb);
-                    mdv_sub(u, v, acc[r]);
-                }
+                for (int q = 0; q < NQ; q++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        cpx<R> yv[P], o[P];
+                        if (HAS_Y) IO::ld(a.y + q * a.stride + (size_t)c * Vh + k, yv);
+#pragma unroll
+                        for (int i = 0; i < P; i++) {
+                            const cpx<R> A = acc[q * P + i].c[c];
+                            if (HAS_Y) {
+                                const R al = a.use_alphas ? a.alphas[q * P + i] : a.alpha;
+                                o[i] = mk<R>(dot2(a.beta, A.re, al, yv[i].re), dot2(a.beta, A.im, al, yv[i].im));
+                                if (RED)
+                                    red[q * P + i] += dot2((double)yv[i].re, (double)o[i].re, (double)yv[i].im, (double)o[i].im);
+                            } else {
+                                o[i] = mk<R>(a.beta * A.re, a.beta * A.im);
+                            }
+                        }
+                        IO::st(a.out + q * a.stride + (size_t)c * Vh + k, o);
+                    }
             }
+            if (RED) reduce_tile<NR>(red, a.partials, tile);
+        } else {
+            Site s = site_of(a.g, a.p_out, k < kend ? k : a.k_lo);
+            if (PF && k < kend) {
 #pragma unroll
-            for (int r = 0; r < NR; r++) {
-                vec3<R> o;
-                if (HAS_Y) {
-                    if (PF && r == 0) cp_async_wait_all();
-                    const vec3<R> yv = PF ? S::template load_plain<R>(ysm + r * S::planes * BLOCK, BLOCK, threadIdx.x)
-                                          : S::template load<R>(a.y + r * a.stride, Vh, k);
-                    const R al = a.use_alphas ? a.alphas[r] : a.alpha;
+                for (int r = 0; r < NR; r++)
 #pragma unroll
-                    for (int c = 0; c < 3; c++)
-                        o.c[c] = mk<R>(al * yv.c[c].re + a.beta * acc[r].c[c].re,
-                                       al * yv.c[c].im + a.beta * acc[r].c[c].im);
-                    if (RED) {
+                    for (int pl = 0; pl < S::planes; pl++)
+                        cp_async_elem<sizeof(E)>(&ysm[(r * S::planes + pl) * BLOCK + threadIdx.x],
+                                                 a.y + r * a.stride + (size_t)pl * Vh + k);
+                cp_async_commit();
+            }
+            double red[NR];
+#pragma unroll
+            for (int j = 0; j < NR; j++) red[j] = 0.0;
+
+            if (k < kend) {
+                vec3<R> acc[NR];
+#pragma unroll
+                for (int r = 0; r < NR; r++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) acc[r].c[c] = mk<R>(0, 0);
+#pragma unroll
+                for (int mu = 0; mu < 4; mu++) {
+                    su3m<R> u;
+                    const int kf = neighbour(a.g, s, mu, +1);
+                    a.links.load(mu, a.p_out, k, u, eta_of(a.g, s, mu));
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        vec3<R> v = LF::store::template load<R>(a.in + r * a.stride, Vh, kf);
+                        mv_acc(u, v, acc[r]);
+                    }
+                    const int kb = neighbour(a.g, s, mu, -1);
+                    a.links.load(mu, 1 - a.p_out, kb, u, eta_back(a.g, s, mu));
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        vec3<R> v = LF::store::template load<R>(a.in + r * a.stride, Vh, kb);
+                        mdv_sub(u, v, acc[r]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    vec3<R> o;
+                    if (HAS_Y) {
+                        if (PF && r == 0) cp_async_wait_all();
+                        const vec3<R> yv = PF ? S::template load_plain<R>(ysm + r * S::planes * BLOCK, BLOCK, threadIdx.x)
+                                              : S::template load<R>(a.y + r * a.stride, Vh, k);
+                        const R al = a.use_alphas ? a.alphas[r] : a.alpha;
 #pragma unroll
                         for (int c = 0; c < 3; c++)
-                            red[r] += (double)yv.c[c].re * (double)o.c[c].re + (double)yv.c[c].im * (double)o.c[c].im;
-                    }
-                } else {
+                            o.c[c] = mk<R>(dot2(a.beta, acc[r].c[c].re, al, yv.c[c].re),
+                                           dot2(a.beta, acc[r].c[c].im, al, yv.c[c].im));
+                        if (RED) {
 #pragma unroll
-                    for (int c = 0; c < 3; c++) o.c[c] = mk<R>(a.beta * acc[r].c[c].re, a.beta * acc[r].c[c].im);
+                            for (int c = 0; c < 3; c++)
+                                red[r] += dot2((double)yv.c[c].re, (double)o.c[c].re, (double)yv.c[c].im, (double)o.c[c].im);
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 3; c++) o.c[c] = mk<R>(a.beta * acc[r].c[c].re, a.beta * acc[r].c[c].im);
+                    }
+                    LF::store::template store<R>(a.out + r * a.stride, Vh, k, o);
                 }
-                LF::store::template store<R>(a.out + r * a.stride, Vh, k, o);
             }
+            if (RED)
+                reduce_tile<NR>(red, a.partials, tile);  // ends with a barrier
+            else if (PF)
+                __syncthreads();  // ysm is refilled by the next tile
         }
-        if (RED)
-            reduce_tile<NR>(red, a.partials, tile);  // ends with a barrier
-        else if (PF)
-            __syncthreads();  // ysm is refilled by the next tile
     }
     if (RED) reduce_last<NR>(a.partials, a.ticket, ntiles * (BLOCK / RED_CHUNK), a.fin);
 }
@@ -197,8 +266,8 @@ inline void dslash_launch_cand(int cand, const DslashArgs<LF, NR, FIN> &a, int n
 template <class LF, int NR, bool HAS_Y, bool RED>
 inline std::string dslash_tune_name()
 {
-    return std::string("dslash ") + LF::name + " nr=" + std::to_string(NR) + " y=" + std::to_string((int)HAS_Y) +
-           " red=" + std::to_string((int)RED);
+    return std::string("dslash ") + LF::name + (LF::store::pack > 1 ? " pack=" + std::to_string(LF::store::pack) : "") +
+           " nr=" + std::to_string(NR) + " y=" + std::to_string((int)HAS_Y) + " red=" + std::to_string((int)RED);
 }
 
 // Times the three candidates of an instantiation on scratch spinors (the caller's links) with

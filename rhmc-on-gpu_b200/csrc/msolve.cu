@@ -3,6 +3,7 @@
 // precision schedule with reliable updates, and the FP64 true residuals.
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "capi_util.h"
@@ -122,26 +123,30 @@ static int ms_phase(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo *
         CK(cudaGetLastError());
     }
 
-    // D_oe and D_eo launch arguments
-    DslashArgs<LF, NR, NoFin> a1;
+    // D_oe and D_eo launch arguments, on the base vectors' packed layout (BasePack)
+    typedef typename std::conditional<BasePack<Rv, NR>::P == 1, LF, LPack<LF, BasePack<Rv, NR>::P>>::type LFB;
+    typedef typename LFB::store::elem EB;
+    LFB lfb;
+    static_cast<LF &>(lfb) = lf;
+    DslashArgs<LFB, NR, NoFin> a1;
     memset(&a1, 0, sizeof(a1));
     a1.g = c->g;
     a1.p_out = 1;
-    a1.links = lf;
-    a1.in = (const E *)p;
-    a1.out = (E *)h;
+    a1.links = lfb;
+    a1.in = (const EB *)p;
+    a1.out = (EB *)h;
     a1.stride = stride;
     a1.beta = (Rv)0.5;
     a1.stop = &st->stop;
     a1.stop_set = &st->stop_k4;
-    DslashArgs<LF, NR, FinAlpha<NR>> a2;
+    DslashArgs<LFB, NR, FinAlpha<NR>> a2;
     memset(&a2, 0, sizeof(a2));
     a2.g = c->g;
     a2.p_out = 0;
-    a2.links = lf;
-    a2.in = (const E *)h;
-    a2.out = (E *)s;
-    a2.y = (const E *)p;
+    a2.links = lfb;
+    a2.in = (const EB *)h;
+    a2.out = (EB *)s;
+    a2.y = (const EB *)p;
     a2.stride = stride;
     a2.alpha = (Rv)(c->mass * c->mass + A.base[0]);
     a2.use_alphas = 1;  // every RHS iterates its own base operator M^dag M + base[r]
@@ -183,8 +188,8 @@ static int ms_phase(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo *
     } key;
     memset(&key, 0, sizeof(key));
     // launch shapes (tuned now, outside the capture, when unknown)
-    key.cand[0] = dslash_candidate<LF, NR, false, false>(c->g, lf, s_);
-    key.cand[1] = dslash_candidate<LF, NR, true, true>(c->g, lf, s_);
+    key.cand[0] = dslash_candidate<LFB, NR, false, false>(c->g, lfb, s_);
+    key.cand[1] = dslash_candidate<LFB, NR, true, true>(c->g, lfb, s_);
     if (ru) {
         key.cand[2] = dslash_candidate<L64_12, NR, false, false>(c->g, l64, s_);
         key.cand[3] = dslash_candidate<L64_12, NR, true, false>(c->g, l64, s_);
@@ -203,8 +208,8 @@ static int ms_phase(rhmc_ctx *c, const LF &lf, const MSolveArgs &A, MSolveInfo *
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
         for (int it = 0; it < chunk; it++) {
-            dslash_launch_cand<LF, NR, false, false, NoFin>(key.cand[0], a1, Vh, s_);
-            dslash_launch_cand<LF, NR, true, true, FinAlpha<NR>>(key.cand[1], a2, Vh, s_);
+            dslash_launch_cand<LFB, NR, false, false, NoFin>(key.cand[0], a1, Vh, s_);
+            dslash_launch_cand<LFB, NR, true, true, FinAlpha<NR>>(key.cand[1], a2, Vh, s_);
             ms_resid_kernel<Rv, NR><<<persistent_grid((const void *)ms_resid_kernel<Rv, NR>, VEC_BLOCK, gv), VEC_BLOCK, 0,
                                       s_>>>(Vh, stride, (E *)r, (const E *)s, pt, tk + 2, st);
             ms_update_kernel<Rv, NR><<<gv, VEC_BLOCK, 0, s_>>>(Vh, stride, (const E *)r, (E *)p, st);

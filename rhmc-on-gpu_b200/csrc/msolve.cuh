@@ -232,6 +232,24 @@ struct MSVec {
     typedef typename SpinorT<Rv>::elem E;
 };
 
+// Layout of the base vectors (residual ring, p, h, s) of NR right-hand sides in precision Rv:
+// packed P at a time (PackS; 32-byte elements: 4 FP32 or 2 FP64 right-hand sides of one colour
+// and site), so that the Dslash of the batch loads P right-hand sides per instruction; plane per
+// RHS (P = 1) when NR does not split into such packs.  The shifted solutions and directions, the
+// right-hand sides b and every caller-visible vector keep the plane layout.
+template <typename Rv, int NR>
+struct BasePack {
+    static constexpr int P = sizeof(Rv) == 4 ? (NR % 4 == 0 ? 4 : (NR % 2 == 0 ? 2 : 1)) : (NR % 2 == 0 ? 2 : 1);
+};
+
+// index, in complex numbers, of RHS j, colour c, site k in a set of NR base vectors
+template <typename Rv, int NR>
+__host__ __device__ __forceinline__ size_t bidx(int j, int c, int k, int Vh)
+{
+    constexpr int P = BasePack<Rv, NR>::P;
+    return ((size_t)((j / P) * 3 + c) * Vh + k) * P + (j % P);
+}
+
 // x_i = 0, r_0 = p = p_i = b (b FP64 internal), |b|^2.  r_0 goes to the last slot of the
 // residual ring (the slot the first iteration reads).  Base vectors (ring, p) are stored in Rv,
 // the shifted solutions and directions (x, ps) in Rx.
@@ -253,14 +271,14 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_init_kernel(int Vh, int nshift, 
         for (int j = 0; j < NR; j++) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const size_t o = j * stride + (size_t)c * Vh + k;
+                const size_t o = j * stride + (size_t)c * Vh + k, ob = bidx<Rv, NR>(j, c, k, Vh);
                 const double2 v = b[o];
-                red[j] += v.x * v.x + v.y * v.y;
+                red[j] += dot2(v.x, v.x, v.y, v.y);
                 E e;
                 e.x = (Rv)v.x;
                 e.y = (Rv)v.y;
-                r[o] = e;
-                p[o] = e;
+                r[ob] = e;
+                p[ob] = e;
                 EX ex, z;
                 ex.x = (Rx)v.x;
                 ex.y = (Rx)v.y;
@@ -298,6 +316,9 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_resid_kernel(int Vh, size_t stri
     }
     // tiles of VEC_BLOCK sites walked by a persistent grid (persistent_grid), so the reduction's
     // per-block fence and ticket are paid once per block
+    constexpr int P = BasePack<Rv, NR>::P;
+    typedef PackIO<Rv, P> IO;
+    typedef PackElem<Rv, P> PE;
     const int ntiles = (Vh + VEC_BLOCK - 1) / VEC_BLOCK;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int k = tile * VEC_BLOCK + threadIdx.x;
@@ -306,17 +327,33 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_resid_kernel(int Vh, size_t stri
         for (int j = 0; j < NR; j++) red[j] = 0.0;
         if (k < Vh) {
 #pragma unroll
-            for (int j = 0; j < NR; j++) {
-                if (!run[j]) continue;
+            for (int q = 0; q < NR / P; q++) {
+                int any = 0, all = 1;
+#pragma unroll
+                for (int i = 0; i < P; i++) {
+                    any |= run[q * P + i];
+                    all &= run[q * P + i];
+                }
+                if (!any) continue;
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
-                    const size_t o = j * stride + (size_t)c * Vh + k;
-                    E rv = rprev[o];
-                    const E sv = s[o];
-                    rv.x = rv.x + om[j] * sv.x;
-                    rv.y = rv.y + om[j] * sv.y;
-                    r[o] = rv;
-                    red[j] += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+                    const size_t o = bidx<Rv, NR>(q * P, c, k, Vh) / P;  // pack element
+                    cpx<Rv> rv[P], sv[P], keep[P];
+                    IO::ld((const PE *)rprev + o, rv);
+                    IO::ld((const PE *)s + o, sv);
+                    if (!all) IO::ldc((const PE *)r + o, keep);  // a stopped RHS keeps its slot
+#pragma unroll
+                    for (int i = 0; i < P; i++) {
+                        const int j = q * P + i;
+                        if (run[j]) {
+                            rv[i].re = rv[i].re + om[j] * sv[i].re;
+                            rv[i].im = rv[i].im + om[j] * sv[i].im;
+                            red[j] += dot2((double)rv[i].re, (double)rv[i].re, (double)rv[i].im, (double)rv[i].im);
+                        } else {
+                            rv[i] = keep[i];
+                        }
+                    }
+                    IO::st((PE *)r + o, rv);
                 }
             }
         }
@@ -333,23 +370,37 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_update_kernel(int Vh, size_t str
                                                                typename MSVec<Rv>::E *p, MSState *st)
 {
     typedef typename MSVec<Rv>::E E;
+    constexpr int P = BasePack<Rv, NR>::P;
+    typedef PackIO<Rv, P> IO;
+    typedef PackElem<Rv, P> PE;
     if (*(volatile int *)&st->stop_k4) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= Vh) return;
     const E *r = ring + (size_t)((*(volatile const int *)&st->wpos + MS_WIN - 1) % MS_WIN) * NR * stride;
 #pragma unroll
-    for (int j = 0; j < NR; j++) {
-        const MSRhs &q = st->rhs[j];
-        if (!q.running) continue;
-        const Rv g = (Rv)q.gamma;
+    for (int q = 0; q < NR / P; q++) {
+        int run[P], any = 0;
+        Rv g[P];
+#pragma unroll
+        for (int i = 0; i < P; i++) {
+            run[i] = st->rhs[q * P + i].running;
+            g[i] = (Rv)st->rhs[q * P + i].gamma;
+            any |= run[i];
+        }
+        if (!any) continue;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const size_t o = j * stride + (size_t)c * Vh + k;
-            const E rv = r[o];
-            E pv = p[o];
-            pv.x = rv.x + g * pv.x;
-            pv.y = rv.y + g * pv.y;
-            p[o] = pv;
+            const size_t o = bidx<Rv, NR>(q * P, c, k, Vh) / P;  // pack element
+            cpx<Rv> rv[P], pv[P];
+            IO::ld((const PE *)r + o, rv);
+            IO::ldc((const PE *)p + o, pv);
+#pragma unroll
+            for (int i = 0; i < P; i++)
+                if (run[i]) {  // a stopped RHS keeps its direction
+                    pv[i].re = rv[i].re + g[i] * pv[i].re;
+                    pv[i].im = rv[i].im + g[i] * pv[i].im;
+                }
+            IO::st((PE *)p + o, pv);
         }
     }
 }
@@ -399,43 +450,54 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_flush_kernel(int Vh, int nshift,
         s_use[t] = any ? (q.active_next[i] ? 2 : 1) : 0;
     }
     __syncthreads();
+    constexpr int P = BasePack<Rv, NR>::P;
+    typedef PackIO<Rv, P> IO;
+    typedef PackElem<Rv, P> PE;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < Vh && wp > 0) {
-        for (int j = 0; j < NR; j++) {
+        for (int q = 0; q < NR / P; q++) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                // the window's residuals of this site, read once and shared by every shift
-                E rv[MS_WIN];
+                // the window's residuals of this site, read once (a pack of P right-hand sides per
+                // load) and shared by every shift
+                cpx<Rv> rp[MS_WIN][P];
 #pragma unroll
                 for (int m = 0; m < MS_WIN; m++)
-                    if (m < wp) {
-                        const typename MSVec<Rv>::E q = ring[((size_t)m * NR + j) * stride + (size_t)c * Vh + k];
-                        rv[m].x = (Rx)q.x;
-                        rv[m].y = (Rx)q.y;
-                    }
-                for (int i = 0; i < nshift; i++) {
-                    const int t = j * nshift + i, use = s_use[t];
-                    if (!use) continue;
-                    const size_t o = (size_t)t * stride + (size_t)c * Vh + k;
-                    const Rx x0 = (Rx)s_cx0[t], a0 = (Rx)s_ca[t];
-                    const E p0 = ps[o];
-                    E xv = x[o];
-                    E pv;
-                    xv.x = xv.x - x0 * p0.x;
-                    xv.y = xv.y - x0 * p0.y;
-                    pv.x = a0 * p0.x;
-                    pv.y = a0 * p0.y;
+                    if (m < wp) IO::ld((const PE *)(ring + (size_t)m * NR * stride) + bidx<Rv, NR>(q * P, c, k, Vh) / P, rp[m]);
 #pragma unroll
-                    for (int m = 0; m < MS_WIN; m++) {
-                        if (m >= wp) break;
-                        const Rx cx = (Rx)s_cx[t][m], cb = (Rx)s_cb[t][m];
-                        xv.x = xv.x - cx * rv[m].x;
-                        xv.y = xv.y - cx * rv[m].y;
-                        pv.x = pv.x + cb * rv[m].x;
-                        pv.y = pv.y + cb * rv[m].y;
+                for (int l = 0; l < P; l++) {
+                    const int j = q * P + l;
+                    E rv[MS_WIN];
+#pragma unroll
+                    for (int m = 0; m < MS_WIN; m++)
+                        if (m < wp) {
+                            rv[m].x = (Rx)rp[m][l].re;
+                            rv[m].y = (Rx)rp[m][l].im;
+                        }
+                    for (int i = 0; i < nshift; i++) {
+                        const int t = j * nshift + i, use = s_use[t];
+                        if (!use) continue;
+                        const size_t o = (size_t)t * stride + (size_t)c * Vh + k;
+                        const Rx x0 = (Rx)s_cx0[t], a0 = (Rx)s_ca[t];
+                        const E p0 = ps[o];
+                        E xv = x[o];
+                        E pv;
+                        xv.x = xv.x - x0 * p0.x;
+                        xv.y = xv.y - x0 * p0.y;
+                        pv.x = a0 * p0.x;
+                        pv.y = a0 * p0.y;
+#pragma unroll
+                        for (int m = 0; m < MS_WIN; m++) {
+                            if (m >= wp) break;
+                            const Rx cx = (Rx)s_cx[t][m], cb = (Rx)s_cb[t][m];
+                            xv.x = xv.x - cx * rv[m].x;
+                            xv.y = xv.y - cx * rv[m].y;
+                            pv.x = pv.x + cb * rv[m].x;
+                            pv.y = pv.y + cb * rv[m].y;
+                        }
+                        x[o] = xv;
+                        if (use == 2) ps[o] = pv;
                     }
-                    x[o] = xv;
-                    if (use == 2) ps[o] = pv;
                 }
             }
         }
@@ -492,15 +554,15 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_convert_kernel(int Vh, size_t st
         const int slot = st->rhs[j].rslot;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const size_t o = j * stride + (size_t)c * Vh + k;
-            const typename MSVec<Rf>::E rv = ring_f[(size_t)slot * NR * stride + o], pv = p_f[o];
+            const size_t of = bidx<Rf, NR>(j, c, k, Vh), ot = bidx<Rt, NR>(j, c, k, Vh);
+            const typename MSVec<Rf>::E rv = ring_f[(size_t)slot * NR * stride + of], pv = p_f[of];
             typename MSVec<Rt>::E a, b;
             a.x = (Rt)rv.x;
             a.y = (Rt)rv.y;
             b.x = (Rt)pv.x;
             b.y = (Rt)pv.y;
-            ring_t[(size_t)(MS_WIN - 1) * NR * stride + o] = a;
-            p_t[o] = b;
+            ring_t[(size_t)(MS_WIN - 1) * NR * stride + ot] = a;
+            p_t[ot] = b;
         }
     }
 }
@@ -593,17 +655,17 @@ __global__ void __launch_bounds__(VEC_BLOCK) ms_ru_resid_kernel(int Vh, int nshi
             const size_t pbase = (size_t)(j * nshift + st->rhs[j].i0) * stride;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const size_t o = j * stride + (size_t)c * Vh + k;
+                const size_t o = j * stride + (size_t)c * Vh + k, ob = bidx<Rv, NR>(j, c, k, Vh);
                 const double2 bv = b[o], tv = t[o], pv = ps[pbase + (size_t)c * Vh + k];
                 const double re = bv.x - tv.x, im = bv.y - tv.y;
-                red[j] += re * re + im * im;
+                red[j] += dot2(re, re, im, im);
                 E e, f;
                 e.x = (Rv)re;
                 e.y = (Rv)im;
                 f.x = (Rv)pv.x;
                 f.y = (Rv)pv.y;
-                ring[(size_t)(MS_WIN - 1) * NR * stride + o] = e;
-                p[o] = f;
+                ring[(size_t)(MS_WIN - 1) * NR * stride + ob] = e;
+                p[ob] = f;
             }
         }
     }

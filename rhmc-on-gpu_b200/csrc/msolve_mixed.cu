@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_resid_kernel(int Vh, size_t stri
                 const size_t o = j * stride + (size_t)c * Vh + k;
                 const double2 bv = b[o], xv = x[o], tv = t[o];
                 const double re = bv.x - co.coef[j] * xv.x - tv.x, im = bv.y - co.coef[j] * xv.y - tv.y;
-                red[j] += re * re + im * im;
+                red[j] += dot2(re, re, im, im);
                 r.c[c] = mk<double>(re, im);
             }
             S::template store<double>(rs + j * sstride, Vh, k, r);
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(VEC_BLOCK) rb_xr_kernel(int Vh, size_t stride,
                     xs[o] = xv;
                     rv.c[c].re -= a * av.c[c].re;
                     rv.c[c].im -= a * av.c[c].im;
-                    red[j] += (double)rv.c[c].re * rv.c[c].re + (double)rv.c[c].im * rv.c[c].im;
+                    red[j] += dot2((double)rv.c[c].re, (double)rv.c[c].re, (double)rv.c[c].im, (double)rv.c[c].im);
                 }
                 S::template store<Rs>(rs + j * sstride, Vh, k, rv);
             }

@@ -292,6 +292,7 @@ struct F64S {
     typedef double2 elem;
     static constexpr int planes = 3;
     static constexpr bool soa = true;  // plane c of site k at c * Vh + k
+    static constexpr int pack = 1;    // right-hand sides per element (PackS)
     template <typename R>
     __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int Vh, int k)
     {
@@ -328,6 +329,7 @@ struct F32S {
     typedef float2 elem;
     static constexpr int planes = 3;
     static constexpr bool soa = true;
+    static constexpr int pack = 1;
     template <typename R>
     __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int Vh, int k)
     {
@@ -366,6 +368,7 @@ struct A64S {
     typedef double2 elem;
     static constexpr int planes = 3;
     static constexpr bool soa = false;
+    static constexpr int pack = 1;
     template <typename R>
     __device__ __forceinline__ static vec3<R> load(const elem *__restrict__ v, int, int k)
     {
@@ -405,6 +408,7 @@ struct H16S {
     typedef uint4 elem;
     static constexpr int planes = 1;
     static constexpr bool soa = true;
+    static constexpr int pack = 1;
     __device__ __forceinline__ static float2 h2f(unsigned w) { return __half22float2(*reinterpret_cast<const __half2 *>(&w)); }
     __device__ __forceinline__ static unsigned f2h(float a, float b)
     {
@@ -465,6 +469,126 @@ __device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// ------------------------------------------------------------------ packed right-hand sides
+// A batch of right-hand sides stored P at a time: element (pack q, colour c, site k) holds the P
+// complex numbers of RHS qP .. qP+P-1 contiguously at element index (q*3 + c)*Vh + k, consecutive
+// packs `stride` elements apart (stride >= 3 Vh).  One 16- or 32-byte load then brings P
+// right-hand sides of a colour and site, where one-plane-per-RHS storage needs P 8- or 16-byte
+// loads: fewer load instructions, more bytes in flight per instruction.  (P = 1 is the plane
+// layout of F64S / F32S.)
+template <typename R, int P> struct __align__(P * 2 * sizeof(R)) PackElem { R v[2 * P]; };
+
+template <typename R, int P> struct PackIO;
+// ld: read-only path (data the kernel does not write); ldc: coherent load (read-modify-write)
+template <typename R> struct PackIO<R, 1> {
+    __device__ __forceinline__ static void ld(const PackElem<R, 1> *e, cpx<R> (&o)[1])
+    {
+        const typename SpinorT<R>::elem a = __ldg(reinterpret_cast<const typename SpinorT<R>::elem *>(e));
+        o[0] = mk<R>(a.x, a.y);
+    }
+    __device__ __forceinline__ static void ldc(const PackElem<R, 1> *e, cpx<R> (&o)[1])
+    {
+        const typename SpinorT<R>::elem a = *reinterpret_cast<const typename SpinorT<R>::elem *>(e);
+        o[0] = mk<R>(a.x, a.y);
+    }
+    __device__ __forceinline__ static void st(PackElem<R, 1> *e, const cpx<R> (&o)[1])
+    {
+        typename SpinorT<R>::elem a;
+        a.x = o[0].re;
+        a.y = o[0].im;
+        *reinterpret_cast<typename SpinorT<R>::elem *>(e) = a;
+    }
+};
+template <> struct PackIO<float, 2> {
+    __device__ __forceinline__ static void ld(const PackElem<float, 2> *e, cpx<float> (&o)[2])
+    {
+        const float4 a = __ldg(reinterpret_cast<const float4 *>(e));
+        o[0] = mk<float>(a.x, a.y);
+        o[1] = mk<float>(a.z, a.w);
+    }
+    __device__ __forceinline__ static void ldc(const PackElem<float, 2> *e, cpx<float> (&o)[2])
+    {
+        const float4 a = *reinterpret_cast<const float4 *>(e);
+        o[0] = mk<float>(a.x, a.y);
+        o[1] = mk<float>(a.z, a.w);
+    }
+    __device__ __forceinline__ static void st(PackElem<float, 2> *e, const cpx<float> (&o)[2])
+    {
+        *reinterpret_cast<float4 *>(e) = make_float4(o[0].re, o[0].im, o[1].re, o[1].im);
+    }
+};
+template <> struct PackIO<float, 4> {  // 32-byte accesses (sm_100)
+    __device__ __forceinline__ static void ld(const PackElem<float, 4> *e, cpx<float> (&o)[4])
+    {
+        float a[8];
+        asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(a[4]), "=f"(a[5]), "=f"(a[6]), "=f"(a[7])
+                     : "l"(e));
+#pragma unroll
+        for (int i = 0; i < 4; i++) o[i] = mk<float>(a[2 * i], a[2 * i + 1]);
+    }
+    __device__ __forceinline__ static void ldc(const PackElem<float, 4> *e, cpx<float> (&o)[4])
+    {
+        float a[8];
+        asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(a[4]), "=f"(a[5]), "=f"(a[6]), "=f"(a[7])
+                     : "l"(e)
+                     : "memory");
+#pragma unroll
+        for (int i = 0; i < 4; i++) o[i] = mk<float>(a[2 * i], a[2 * i + 1]);
+    }
+    __device__ __forceinline__ static void st(PackElem<float, 4> *e, const cpx<float> (&o)[4])
+    {
+        asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(e), "f"(o[0].re), "f"(o[0].im), "f"(o[1].re),
+                     "f"(o[1].im), "f"(o[2].re), "f"(o[2].im), "f"(o[3].re), "f"(o[3].im)
+                     : "memory");
+    }
+};
+template <> struct PackIO<double, 2> {  // 32-byte accesses (sm_100)
+    __device__ __forceinline__ static void ld(const PackElem<double, 2> *e, cpx<double> (&o)[2])
+    {
+        double a[4];
+        asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a[0]), "=d"(a[1]), "=d"(a[2]), "=d"(a[3]) : "l"(e));
+        o[0] = mk<double>(a[0], a[1]);
+        o[1] = mk<double>(a[2], a[3]);
+    }
+    __device__ __forceinline__ static void ldc(const PackElem<double, 2> *e, cpx<double> (&o)[2])
+    {
+        double a[4];
+        asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a[0]), "=d"(a[1]), "=d"(a[2]), "=d"(a[3]) : "l"(e) : "memory");
+        o[0] = mk<double>(a[0], a[1]);
+        o[1] = mk<double>(a[2], a[3]);
+    }
+    __device__ __forceinline__ static void st(PackElem<double, 2> *e, const cpx<double> (&o)[2])
+    {
+        asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(e), "d"(o[0].re), "d"(o[0].im), "d"(o[1].re), "d"(o[1].im)
+                     : "memory");
+    }
+};
+
+// storage policy of packed spinors (the Dslash kernel reads and writes whole packs)
+template <typename R, int P>
+struct PackS {
+    typedef R real;
+    typedef PackElem<R, P> elem;
+    static constexpr int planes = 3;
+    static constexpr bool soa = true;
+    static constexpr int pack = P;
+};
+
+// a link format whose spinors are packed P right-hand sides at a time
+template <class L, int P>
+struct LPack : L {
+    typedef PackS<typename L::real, P> store;
+};
+
+// a*b + c*d rounded one fixed way, fma(a, b, c*d).  Left to the compiler's FMA contraction, an
+// expression with two products may fuse either one, and the choice can differ between template
+// instantiations: results that must be bit-identical across batch widths, launch shapes and
+// storage layouts (reductions, the Dslash epilogue) use this instead.
+__device__ __forceinline__ double dot2(double a, double b, double c, double d) { return __fma_rn(a, b, __dmul_rn(c, d)); }
+__device__ __forceinline__ float dot2(float a, float b, float c, float d) { return __fmaf_rn(a, b, __fmul_rn(c, d)); }
 
 // ------------------------------------------------------------------ SU(3) x vector
 // acc += U v

@@ -134,6 +134,13 @@ int main(int argc, char **argv)
     sweep<L32_12, 1, false>("f32_12", f12);
     sweep<L32_12, 4, false>("f32_12", f12);
     sweep<L32_12, 4, true>("f32_12", f12);
+    // the solvers' base vectors: right-hand sides packed 4 (FP32) or 2 (FP64) per 32-byte element
+    LPack<L32_12, 4> f12q; f12q.p = f12.p; f12q.Vh = f12.Vh;
+    LPack<L64_12, 2> l12p; l12p.p = l12.p; l12p.Vh = l12.Vh;
+    sweep<LPack<L32_12, 4>, 4, false>("f32_12q", f12q);
+    sweep<LPack<L32_12, 4>, 4, true>("f32_12q", f12q);
+    sweep<LPack<L64_12, 2>, 4, false>("f64_12p", l12p);
+    sweep<LPack<L64_12, 2>, 4, true>("f64_12p", l12p);
     sweep<L32_12, 8, false>("f32_12", f12);
     sweep<L32_12, 8, true>("f32_12", f12);
     sweep<L32_18, 1, false>("f32_18", f18);

@@ -3,7 +3,8 @@ lib/Action/Inverter/inverter.cc:142-339) and against the reference's own CPU cod
 
 Tolerances: FP64 mode reproduces the reference iteration (same recurrences, FP64, FMA
 rounding only), so solutions agree to 1e-10 relative at residual 1e-10; mixed mode is checked
-by the FP64 true residual of every system, which must be <= the requested residual.
+by the FP64 true residual of every system, which must be <= the requested residual (up to the
+rounding of its evaluation, 1e-3 of it at 1e-10).
 """
 import numpy as np
 import pytest
@@ -98,11 +99,13 @@ def test_msolve_mixed_true_residual(fmt, nrhs, oracle_mod):
     assert info["systems_refined"] <= 2 * nrhs, info
     xm = xm.reshape(nrhs, len(shifts), ctx.Vh, 3)
     # FP64 true residuals through the library and through the oracle operator
+    # (the library certifies its own FP64 evaluation of |b - A x| <= res; the oracle's evaluation
+    # rounds differently, by about 1e-16 |b| per component: ~3e-14 absolute here, 3e-4 of res)
     orc = oracle_mod.Oracle(dims)
     for r in range(nrhs):
         for i, s in enumerate(shifts):
             rr = bs[r] - orc.mdagm(u, xm[r, i], mass, s)
-            assert np.linalg.norm(rr) <= res * 1.0000001, (r, i, np.linalg.norm(rr))
+            assert np.linalg.norm(rr) <= res * (1 + 1e-3), (r, i, np.linalg.norm(rr))
     xf, _ = ctx.msolve_host(bs if nrhs > 1 else bs[0], shifts, res)
     xf = xf.reshape(nrhs, len(shifts), ctx.Vh, 3)
     assert rel_err(xm, xf) < 1e-8
@@ -183,5 +186,5 @@ def test_msolve_pole_set_per_rhs(mode, fmt, oracle_mod):
             assert np.array_equal(x1, xb[r])
         for i, sg in enumerate(sets[r]):
             rr = bs[r] - orc.mdagm(u, xb[r, i], mass, sg)
-            if mode == rb.MSOLVE_MIXED:
-                assert np.linalg.norm(rr) <= res * 1.0000001, (r, i, np.linalg.norm(rr))
+            if mode == rb.MSOLVE_MIXED:  # certified by the library's own FP64 evaluation (see above)
+                assert np.linalg.norm(rr) <= res * (1 + 1e-3), (r, i, np.linalg.norm(rr))
