@@ -233,13 +233,15 @@ struct MSVec {
 };
 
 // Layout of the base vectors (residual ring, p, h, s) of NR right-hand sides in precision Rv:
-// packed P at a time (PackS; 32-byte elements: 4 FP32 or 2 FP64 right-hand sides of one colour
-// and site), so that the Dslash of the batch loads P right-hand sides per instruction; plane per
-// RHS (P = 1) when NR does not split into such packs.  The shifted solutions and directions, the
-// right-hand sides b and every caller-visible vector keep the plane layout.
+// FP32 packed P at a time (PackS; a 32-byte element holds 4 right-hand sides of one colour and
+// site, 16 bytes 2 of them), so that the Dslash of the batch loads P right-hand sides per
+// instruction; plane per RHS (P = 1) for FP64, whose 16-byte plane loads are already wide (its
+// packed form, 2 per 32 bytes, was faster for 4 right-hand sides at 32^4 but slower for 2 and 8
+// in trajectories), and for batch widths that do not split into packs.  The shifted solutions
+// and directions, the right-hand sides b and every caller-visible vector keep the plane layout.
 template <typename Rv, int NR>
 struct BasePack {
-    static constexpr int P = sizeof(Rv) == 4 ? (NR % 4 == 0 ? 4 : (NR % 2 == 0 ? 2 : 1)) : (NR % 2 == 0 ? 2 : 1);
+    static constexpr int P = sizeof(Rv) == 4 ? (NR % 4 == 0 ? 4 : (NR % 2 == 0 ? 2 : 1)) : 1;
 };
 
 // index, in complex numbers, of RHS j, colour c, site k in a set of NR base vectors
