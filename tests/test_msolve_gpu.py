@@ -77,6 +77,24 @@ def test_msolve_batched_rhs_identical():
         assert np.array_equal(x1, xb[r])
 
 
+@pytest.mark.parametrize("nrhs", [2, 4])
+def test_msolve_fp32_packed_batch_identical(nrhs):
+    """FP32 mode keeps a batch's base vectors packed (2 or 4 right-hand sides per element) and a
+    single right-hand side's in plane layout: the two layouts run the same arithmetic per RHS,
+    so each batched solution equals its single solve bit for bit."""
+    from gpu_util import new_ctx
+    dims = (6, 4, 4, 8)
+    ctx = new_ctx(dims, mass=0.05)
+    ctx.set_gauge(F.random_links(dims, seed=125))
+    bs = F.random_spinor(dims, seed=126, n=nrhs)
+    shifts = shifts_log(5, 1e-3, 2.0)
+    xb, info = ctx.msolve_host(bs, shifts, 1e-5, mode=rb.MSOLVE_FP32, fmt=rb.LINKS_F32_12)
+    assert info["status"] == 0, info
+    for r in range(nrhs):
+        x1, _ = ctx.msolve_host(bs[r], shifts, 1e-5, mode=rb.MSOLVE_FP32, fmt=rb.LINKS_F32_12)
+        assert np.array_equal(x1, xb[r]), r
+
+
 @pytest.mark.parametrize("fmt", [rb.LINKS_F32_12, rb.LINKS_F32_18, rb.LINKS_F16_12])
 @pytest.mark.parametrize("nrhs", [1, 4, 5])
 def test_msolve_mixed_true_residual(fmt, nrhs, oracle_mod):
