@@ -49,6 +49,17 @@ def approx_report(groups):
             for si, g in enumerate(groups) for j, c in enumerate(g)]
 
 
+def solver_summary(ctx):
+    """What the driver's solves of the last trajectory cost (rhmc_driver_solver_stats), force
+    solves and heatbath/action solves separately; resets the sums."""
+    keys = ("iters_total", "iters_max", "iters_fp64", "ms_reliable_updates", "refine_iters", "systems_refined",
+            "seconds", "seconds_phase_a")
+    md = ctx.driver_solver_stats(0)
+    metro = ctx.driver_solver_stats(1, reset=True)
+    return {"md": {k: (round(md[k], 3) if isinstance(md[k], float) else md[k]) for k in keys},
+            "metro": {k: (round(metro[k], 3) if isinstance(metro[k], float) else metro[k]) for k in keys}}
+
+
 def half_dslash_bytes(fmt, Vh, nrhs=1):
     return Vh * (8 * LINK_BYTES[fmt] + 2 * SPINOR_BYTES[fmt] * nrhs)
 
@@ -554,6 +565,7 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
         ctx.set_gauge(u_traj)
         ctx.set_momenta(P0)
         stream.synchronize()
+        ctx.driver_solver_stats(0, reset=True)
         n0 = ctx.launch_count()
         t0 = time.perf_counter()
         dS, acc = ctx.update(uniform)
@@ -561,7 +573,7 @@ def nf2p1_bench(a, rb, F, np, torch, rank, dev, stream):
         dt = time.perf_counter() - t0
         traj[name] = {"s_per_trajectory": round(dt, 3), "s_md_only": round(t_md, 3), "delta_H": dS, "accepted": acc,
                       "plaquette_proposal": plaq_md, "plaquette_after": ctx.plaquette(),
-                      "gpu_launches": ctx.launch_count() - n0}
+                      "gpu_launches": ctx.launch_count() - n0, "solves": solver_summary(ctx)}
     traj["speedup_mixed_vs_fp64"] = round(traj["fp64"]["s_per_trajectory"] / traj["mixed"]["s_per_trajectory"], 3)
     traj["speedup_mixed_f32_schedule_vs_fp64"] = round(traj["fp64"]["s_per_trajectory"]
                                                        / traj["mixed_f32_schedule"]["s_per_trajectory"], 3)
@@ -649,16 +661,18 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
         ctx.set_gauge(u0)
         ctx.set_momenta(P0)
         stream.synchronize()
+        ctx.driver_solver_stats(0, reset=True)
         n0 = ctx.launch_count()
         t0 = time.perf_counter()
         dS, acc = ctx.update(uniform)
         stream.synchronize()
         dt = time.perf_counter() - t0
+        solves = solver_summary(ctx)
         free, total = torch.cuda.mem_get_info(dev)
         traj[name] = {"s_per_trajectory": round(dt, 2), "delta_H": dS, "accepted": acc,
                       "plaquette_after": ctx.plaquette(), "gpu_launches": ctx.launch_count() - n0,
                       "workspace_gb": round(ctx.workspace_bytes() / 1e9, 2),
-                      "device_memory_in_use_gb": round((total - free) / 1e9, 2)}
+                      "device_memory_in_use_gb": round((total - free) / 1e9, 2), "solves": solves}
         print("rhmc48: %s trajectory %.1f s, dH %.6g" % (name, dt, dS), file=sys.stderr, flush=True)
     for k in [n for n, *_ in arms[1:]]:
         traj["speedup_%s_vs_fp64_single_rhs" % k] = round(traj["fp64_single_rhs"]["s_per_trajectory"]

@@ -151,7 +151,10 @@ typedef struct {
                               RHMC_LINKS_F16_12 means an FP32 12-real multi-shift phase followed by a
                               refinement whose sloppy CG runs on half links and half spinors) */
     double tol_phase_a;    /* mixed mode, FP32/half fmt: relative residual |r|/|b| at which the FP64
-                              part of the precision schedule hands over to FP32 (0: 1e-3) */
+                              part of the precision schedule hands over to FP32; 0: automatic,
+                              1e-3 |b| but no more than 1e7 x `residual` above the target (the FP32
+                              part leaves the shifted systems near 1e-7 of the hand-over residual)
+                              and no less than 1e-4 |b| */
     double ru_delta;       /* mixed mode: FP32 residual reduction between FP64 updates (0: 0.05) */
     int certify;           /* FP64 mode: afterwards refine, by FP64 CG one system at a time, every system
                               whose FP64 true residual is still above `residual` (the reference's
@@ -328,6 +331,12 @@ int rhmc_update(rhmc_ctx *ctx, double uniform, int *acc, double *delta_s);
 int rhmc_save_conf(rhmc_ctx *ctx);
 int rhmc_copy_saved(rhmc_ctx *ctx);
 int rhmc_driver_stats(rhmc_ctx *ctx, long *force_evals, long *solves);
+/* Sums of the rhmc_msolve_info of every solve the driver ran since rhmc_driver_setup (or the last
+ * reset): which = 0 the force (md) solves, 1 the heatbath and action (metro) solves.  Counts,
+ * iterations and seconds are added up, iters_max is the largest, iters[] holds the last solve's
+ * and status the last error.  No counterpart in the reference (its inverter prints an iteration
+ * count per solve).  reset != 0 zeroes both sums after reading. */
+int rhmc_driver_solver_stats(rhmc_ctx *ctx, int which, rhmc_msolve_info *out, int reset);
 /* Device memory held by the context's workspaces (solver vectors, shifted solutions, driver
  * fields, reduction buffers), in bytes; no counterpart in the reference.  Workspaces grow to
  * the largest request and are kept until rhmc_workspace_release or rhmc_destroy. */

@@ -69,8 +69,36 @@ struct Driver {
     std::vector<Species> sp;  // sp[0]: the context mass with P.no_flavours, P.no_ps
     int cur = 0;              // the species the approx / bounds / phi / chi setters act on
     long force_evals = 0, solves = 0;
+    rhmc_msolve_info sums[2] = {};  // md, metro solves (rhmc_driver_solver_stats)
+    int cat = 1;                    // the sum the next solves go to (0 md, 1 metro)
     std::vector<double> pw_start;  // start vector of the power iterations (auto_bounds)
 };
+
+static void add_info(rhmc_msolve_info &a, const rhmc_msolve_info &b)
+{
+    a.status = b.status ? b.status : a.status;
+    for (int j = 0; j < 8; j++) a.iters[j] = b.iters[j];
+    a.refine_iters += b.refine_iters;
+    a.reliable_updates += b.reliable_updates;
+    a.seconds += b.seconds;
+    a.seconds_phase_a += b.seconds_phase_a;
+    a.systems_refined += b.systems_refined;
+    a.iters_total += b.iters_total;
+    a.iters_max = b.iters_max > a.iters_max ? b.iters_max : a.iters_max;
+    a.iters_fp64 += b.iters_fp64;
+    a.ms_reliable_updates += b.ms_reliable_updates;
+}
+
+// one rhmc_msolve call of the driver, its info added to the md (force) or metro sums
+static int driver_msolve(rhmc_ctx *c, const rhmc_msolve_params *mp, double *x, const double *b)
+{
+    rhmc_msolve_info info;
+    memset(&info, 0, sizeof(info));
+    const int rc = rhmc_msolve(c, mp, x, b, &info);
+    Driver *d = c->driver;
+    add_info(d->sums[d->cat], info);
+    return rc;
+}
 
 static Driver *drv(rhmc_ctx *c) { return c->driver; }
 
@@ -137,13 +165,12 @@ static int solve(rhmc_ctx *c, int s, const Approx &ap, double res, int mode, int
     mp.fmt = fmt;
     if (!d->P.single_rhs) {
         d->solves++;
-        return rhmc_msolve(c, &mp, (double *)x, (const double *)b, nullptr);
+        return driver_msolve(c, &mp, (double *)x, (const double *)b);
     }
     mp.nrhs = 1;
     for (int ps = 0; ps < d->sp[s].no_ps; ps++) {
         d->solves++;
-        const int rc = rhmc_msolve(c, &mp, (double *)(x + (size_t)ps * ap.order * SP(c)), (const double *)(b + (size_t)ps * SP(c)),
-                                   nullptr);
+        const int rc = driver_msolve(c, &mp, (double *)(x + (size_t)ps * ap.order * SP(c)), (const double *)(b + (size_t)ps * SP(c)));
         if (rc) return rc;
     }
     return RHMC_OK;
@@ -248,7 +275,7 @@ static int solve_species(rhmc_ctx *c, int which, const char *in_base, double res
     mp.mode = mode;
     mp.fmt = fmt;
     d->solves++;
-    return rhmc_msolve(c, &mp, (double *)out.x, (const double *)bcat, nullptr);
+    return driver_msolve(c, &mp, (double *)out.x, (const double *)bcat);
 }
 
 // findminmax (findminmax.cc:140-183) on the device, for the current links: FP64 power iterations
@@ -303,6 +330,7 @@ static int inv_approx_calc(rhmc_ctx *c, int which, double res)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
+    d->cat = 1;
     for (int g = 0; g < pole_groups(c, which); g++) {
         Solved sv;
         if ((rc = solve_species(c, which, which == 0 ? "drv_phi" : "drv_chi", res, d->P.metro_mode, d->P.metro_fmt, sv, g)))
@@ -331,6 +359,7 @@ static int fermion_part(rhmc_ctx *c, int add)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
+    d->cat = 0;
     for (int g = 0; g < pole_groups(c, 1); g++) {
         Solved sv;
         if ((rc = solve_species(c, 1, "drv_chi", d->P.residue_md, d->P.md_mode, d->P.md_fmt, sv, g))) return rc;
@@ -353,6 +382,7 @@ static int fermion_action_md(rhmc_ctx *c, double *out)
     int rc = check_ready(c);
     if (rc) return rc;
     Driver *d = drv(c);
+    d->cat = 0;
     double sum = 0.0, v;
     for (int g = 0; g < pole_groups(c, 1); g++) {
         Solved sv;
@@ -607,6 +637,7 @@ int rhmc_driver_setup(rhmc_ctx *c, const rhmc_driver_params *p)
     if (p->pole_group < 0) return fail(RHMC_ERR_ARG, "pole_group must be 0 (all poles at once) or positive");
     Driver *d = ensure_driver(c);
     d->P = *p;
+    memset(d->sums, 0, sizeof(d->sums));
     d->sp[0].no_flavours = p->no_flavours;
     d->sp[0].no_ps = p->no_ps;
     d->configured = true;
@@ -731,6 +762,15 @@ int rhmc_driver_stats(rhmc_ctx *c, long *force_evals, long *solves)
     if (!c || !c->driver) return fail(RHMC_ERR_STATE, "driver not configured");
     if (force_evals) *force_evals = c->driver->force_evals;
     if (solves) *solves = c->driver->solves;
+    return RHMC_OK;
+}
+
+int rhmc_driver_solver_stats(rhmc_ctx *c, int which, rhmc_msolve_info *out, int reset)
+{
+    if (!c || !c->driver) return fail(RHMC_ERR_STATE, "driver not configured");
+    if (which != 0 && which != 1) return fail(RHMC_ERR_ARG, "which must be 0 (md solves) or 1 (metro solves)");
+    if (out) *out = c->driver->sums[which];
+    if (reset) memset(c->driver->sums, 0, sizeof(c->driver->sums));
     return RHMC_OK;
 }
 

@@ -74,6 +74,16 @@ struct MSState {
 };
 
 // ------------------------------------------------------------------ last-block scalar steps
+// The FP32 part of the precision schedule, with its FP64 reliable updates, leaves the shifted
+// systems near 1e-7 of the residual at which it took over (a 1e-10 |b| target is met with the
+// hand-over at 1e-3 |b|): the automatic hand-over (tau < 0) is therefore placed at most this far
+// above the final target, so that deep targets do not leave every system to the refinement.
+constexpr double MS_TAU_REACH = 1e7;
+// ... but not below 1e-4 |b|: targets at the FP64 rounding floor of the smallest poles leave
+// those systems to the refinement whatever the hand-over, and an earlier one only lengthens the
+// FP64 part
+constexpr double MS_TAU_MIN = 1e-4;
+
 struct FinInit {
     MSState *st;
     __device__ void operator()(const double *tot) const
@@ -90,7 +100,12 @@ struct FinInit {
             q.alpha = 0.0;
             q.iter = 0;
             q.rslot = MS_WIN - 1;
-            q.res = st->tau > 0.0 ? fmax(st->res, st->tau * sqrt(tot[r])) : st->res;
+            // precision schedule: the FP64 part ends at tau |b| (tau > 0), or with tau < 0 at
+            // -tau |b| but no more than MS_TAU_REACH above the final target
+            const double nb = sqrt(tot[r]);
+            q.res = st->tau > 0.0   ? fmax(st->res, st->tau * nb)
+                    : st->tau < 0.0 ? fmax(st->res, fmax(MS_TAU_MIN * nb, fmin(-st->tau * nb, MS_TAU_REACH * st->res)))
+                                    : st->res;
             q.running = 1;
             q.running_next = (tot[r] > 0.0) ? 1 : 0;  // b == 0: x = 0 is exact
             if (!isfinite(tot[r])) {

@@ -686,7 +686,9 @@ int rhmc_msolve(rhmc_ctx *c, const rhmc_msolve_params *P, double *x, const doubl
     }
     if (P->mode == RHMC_MSOLVE_MIXED) {
         if (P->fmt < 0 || P->fmt > RHMC_LINKS_F16_12) return fail(RHMC_ERR_ARG, "bad link format %d", P->fmt);
-        const double tolA = P->tol_phase_a > 0 ? P->tol_phase_a : 1e-3;
+        // the hand-over of the precision schedule: the caller's, or 1e-3 |b| but at most
+        // MS_TAU_REACH above the target (negative: automatic)
+        const double tolA = P->tol_phase_a > 0 ? P->tol_phase_a : -1e-3;
         const double rud = (P->ru_delta > 0 && P->ru_delta < 1) ? P->ru_delta : 0.05;
         // batches of 8, 4, 3, 2 or 1 right-hand sides (the widths the kernels are built for)
         const size_t stride = 3 * (size_t)c->Vh;

@@ -18,7 +18,8 @@ struct MSolveArgs {
     const void *b;        // FP64 internal spinors, nrhs of them
     void *x;              // FP64 internal spinors, [nrhs][nshift]
     int fresh = 1;        // 1: start from x = 0; 0: resume the state an FP64 phase left (FP32 links only)
-    double tau = 0.0;     // > 0: stop each RHS once |r| <= tau |b| (to be resumed in lower precision)
+    double tau = 0.0;     // > 0: stop each RHS once |r| <= tau |b| (to be resumed in lower precision);
+                          // < 0: once |r| <= max(1e-4 |b|, min(-tau |b|, 1e7 res)) (FinInit)
     int ru_every = 0;     // > 0: reliable update of the base system every ru_every windows
 };
 

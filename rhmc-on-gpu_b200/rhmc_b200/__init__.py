@@ -439,6 +439,14 @@ def _workspace_bytes(self):
     return n.value
 
 
+def _driver_solver_stats(self, which=0, reset=False):
+    """Sums of the driver's solves since the last reset: which 0 force (md), 1 heatbath/action."""
+    info = MsolveInfo()
+    self.call("rhmc_driver_solver_stats", int(which), ctypes.byref(info), int(bool(reset)))
+    return info.as_dict()
+
+
+Context.driver_solver_stats = _driver_solver_stats
 Context.workspace_bytes = _workspace_bytes
 Context.workspace_release = lambda self: self.call("rhmc_workspace_release")
 

@@ -86,3 +86,28 @@ def test_pole_group_rejects_negative():
     ctx = new_ctx((4, 4, 4, 4))
     with pytest.raises(rb.RhmcError):
         ctx.driver_setup(pole_group=-1)
+
+
+def test_driver_solver_stats():
+    """rhmc_driver_solver_stats sums the driver's solves by kind: heatbath/action solves into one
+    sum, force solves into the other, and resets on request."""
+    from gpu_util import new_ctx
+    g = dict(np.load(os.path.join(HERE, "golden", "ref_t4.npz")))
+    with open(os.path.join(HERE, "golden", "rational_coeffs.json")) as f:
+        cf = json.load(f)["t4"]
+    ctx = new_ctx(tuple(g["dims"]), mass=float(g["mass"]), beta=float(g["beta"]))
+    ctx.set_gauge(g["u"])
+    ctx.driver_setup(no_flavours=2, no_ps=1, residue_md=1e-10, residue_metro=1e-12)
+    for w, c in enumerate(cf):
+        ctx.set_approx(w, c)
+    ctx.set_eig_bounds(*tuple(g["bounds"]))
+    ctx.set_phi(g["phi"])
+    ctx.first_inv_approx_calc(1e-12)
+    md, metro = ctx.driver_solver_stats(0), ctx.driver_solver_stats(1)
+    assert md["iters_total"] == 0 and metro["iters_total"] > 0 and metro["seconds"] > 0
+    ctx.calc_ipdot_fermion()
+    md = ctx.driver_solver_stats(0, reset=True)
+    assert md["iters_total"] > 0 and md["iters_max"] > 0
+    assert ctx.driver_solver_stats(0)["iters_total"] == 0 and ctx.driver_solver_stats(1)["iters_total"] == 0
+    with pytest.raises(rb.RhmcError):
+        ctx.driver_solver_stats(2)
