@@ -643,6 +643,8 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
             ("mixed_batched", rb.MSOLVE_MIXED, rb.LINKS_F64_12, 0, 0),
             ("mixed_batched_f32_schedule", rb.MSOLVE_MIXED, rb.LINKS_F32_12, 0, 0),
             ("mixed_batched_pole_groups_%d" % B5_POLE_GROUP, rb.MSOLVE_MIXED, rb.LINKS_F64_12, 0, B5_POLE_GROUP))
+    only = [v for v in a.b5_arms.split(",") if v]
+    arms = tuple(x for x in arms if not only or x[0] in only)
     for name, mode, fmt, single, pgroup in arms:
         ctx.workspace_release()  # each arm's workspace high-water mark is its own
         ctx.driver_setup(no_flavours=2, no_ps=nps, no_md=a.b5_steps, integrator=rb.INT_LEAPFROG, residue_metro=1e-10,
@@ -674,10 +676,12 @@ def batched_rhmc_bench(a, rb, F, np, torch, rank, dev, stream):
                       "workspace_gb": round(ctx.workspace_bytes() / 1e9, 2),
                       "device_memory_in_use_gb": round((total - free) / 1e9, 2), "solves": solves}
         print("rhmc48: %s trajectory %.1f s, dH %.6g" % (name, dt, dS), file=sys.stderr, flush=True)
-    for k in [n for n, *_ in arms[1:]]:
-        traj["speedup_%s_vs_fp64_single_rhs" % k] = round(traj["fp64_single_rhs"]["s_per_trajectory"]
-                                                          / traj[k]["s_per_trajectory"], 3)
-    traj["delta_H_abs_diff_max"] = max(abs(traj[k]["delta_H"] - traj["fp64_single_rhs"]["delta_H"]) for k, *_ in arms)
+    if "fp64_single_rhs" in traj:
+        for k in [n for n, *_ in arms if n != "fp64_single_rhs"]:
+            traj["speedup_%s_vs_fp64_single_rhs" % k] = round(traj["fp64_single_rhs"]["s_per_trajectory"]
+                                                              / traj[k]["s_per_trajectory"], 3)
+        traj["delta_H_abs_diff_max"] = max(abs(traj[k]["delta_H"] - traj["fp64_single_rhs"]["delta_H"])
+                                           for k, *_ in arms)
     traj["memory_note"] = ("workspace_gb: the library's workspaces after the arm (released before it: solver "
                            "vectors, shifted solutions, driver fields; links, momenta and ipdot come on top); "
                            "device_memory_in_use_gb: the whole device after the arm")
@@ -784,6 +788,7 @@ def main():
     ap.add_argument("--b5-dims", default="48,48,48,48", help="rhmc48 workload: lattice")
     ap.add_argument("--b5-steps", type=int, default=10, help="rhmc48 workload: leapfrog steps per trajectory")
     ap.add_argument("--b5-ps", type=int, default=4, help="rhmc48 workload: pseudofermions per species")
+    ap.add_argument("--b5-arms", default="", help="rhmc48 workload: comma-separated subset of the arms")
     a = ap.parse_args()
     a.warmup = max(3, a.warmup)
     if a.impl == "reference":
