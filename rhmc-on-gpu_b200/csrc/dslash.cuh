@@ -10,8 +10,8 @@
 // Epilogue: out = alpha*y + beta*(2 D in)/2, i.e. beta = +0.5 gives D, beta = -0.5 with
 // alpha = mass^2 + sigma and y = p gives the even-even (M^dag M + sigma) p from D_oe p
 // (lib/Action/Inverter/inverter.cc:206-216).  With RED the kernel also reduces, per RHS,
-// Re<y, out> in FP64 (the <p, A p> of CG) through reduce_finalize, whose fixed summation order
-// makes results reproducible.
+// Re<y, out> in FP64 (the <p, A p> of CG; each site's term formed in the spinors' precision, see
+// site_dot) through reduce_finalize, whose fixed summation order makes results reproducible.
 #pragma once
 #include <cstring>
 #include <string>
@@ -26,13 +26,16 @@ namespace rhmc {
 // blocks of 128 or 256 threads).  A thread
 // carries NR accumulators and NR neighbour spinors, so wide FP64 batches need many registers;
 // the pair trades registers (spills) against resident warps (latency hiding).  The values are
-// the fastest of the sweep in tune/dslash_tune.cu on B200 at 24^3x32 and 32^4.
+// the fastest of the sweep in tune/dslash_tune.cu on B200 at 24^3x32 and 32^4; the one-RHS
+// half-precision kernel, bound by instruction issue, runs fastest with the most resident warps
+// (128 x 6 at 80 registers: 27.4 us at 32^4 against 31 us at 256 x 2).
 template <class LF, int NR, bool RED>
 struct DslashCfg {
     static constexpr bool f64 = sizeof(typename LF::real) == 8;
-    static constexpr bool narrow = f64 && NR >= 3;
+    static constexpr bool half1 = LF::store::planes == 1 && !f64 && NR == 1;  // H16S spinors, one RHS
+    static constexpr bool narrow = (f64 && NR >= 3) || half1;
     static constexpr int block = narrow ? 128 : 256;
-    static constexpr int minb = (f64 && NR >= 8) ? 2 : (narrow ? 3 : 2);
+    static constexpr int minb = half1 ? 6 : ((f64 && NR >= 8) ? 2 : (narrow ? 3 : 2));
 };
 
 // the largest grid any configuration launches (for sizing per-block reduction partials)
@@ -61,6 +64,19 @@ struct DslashArgs {
     const int *run_if;  // optional: skip the launch when *run_if == 0
     int k_lo, k_count;  // output sites [k_lo, k_lo + k_count) (k_count 0: all Vh); no RED with a range
 };
+
+// Re<y, o> of one colour added to a site's term of the fused reduction: FP64 products for FP64
+// spinors; for FP32 spinors the site term is summed in FP32 with fixed rounding and converted to
+// FP64 once per site and RHS (three colours' float-to-double conversions and FP64 products per
+// RHS would cost more issue slots than the whole FP32 epilogue)
+__device__ __forceinline__ void site_dot(double &red, float &, const cpx<double> &y, const cpx<double> &o)
+{
+    red += dot2(y.re, o.re, y.im, o.im);
+}
+__device__ __forceinline__ void site_dot(double &, float &tf, const cpx<float> &y, const cpx<float> &o)
+{
+    tf = __fadd_rn(tf, dot2(y.re, o.re, y.im, o.im));
+}
 
 template <class LF, int NR, bool HAS_Y, bool RED, class FIN, int BLOCK = DslashCfg<LF, NR, RED>::block,
           int MINB = DslashCfg<LF, NR, RED>::minb>
@@ -92,8 +108,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
             static_assert(NR % P == 0, "the batch is a whole number of packs");
             typedef PackIO<R, P> IO;
             double red[NR];
+            float tf[NR];  // FP32 spinors: the site's Re<y, out>, formed in FP32 (site_dot)
 #pragma unroll
-            for (int j = 0; j < NR; j++) red[j] = 0.0;
+            for (int j = 0; j < NR; j++) {
+                red[j] = 0.0;
+                tf[j] = 0.f;
+            }
             if (k < kend) {
                 const Site s = site_of(a.g, a.p_out, k);
                 vec3<R> acc[NR];
@@ -143,14 +163,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
                             if (HAS_Y) {
                                 const R al = a.use_alphas ? a.alphas[q * P + i] : a.alpha;
                                 o[i] = mk<R>(dot2(a.beta, A.re, al, yv[i].re), dot2(a.beta, A.im, al, yv[i].im));
-                                if (RED)
-                                    red[q * P + i] += dot2((double)yv[i].re, (double)o[i].re, (double)yv[i].im, (double)o[i].im);
+                                if (RED) site_dot(red[q * P + i], tf[q * P + i], yv[i], o[i]);
                             } else {
                                 o[i] = mk<R>(a.beta * A.re, a.beta * A.im);
                             }
                         }
                         IO::st(a.out + q * a.stride + (size_t)c * Vh + k, o);
                     }
+                if (RED && sizeof(R) == 4)
+#pragma unroll
+                    for (int j = 0; j < NR; j++) red[j] = (double)tf[j];
             }
             if (RED) reduce_tile<NR>(red, a.partials, tile);
         } else {
@@ -165,8 +187,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
                 cp_async_commit();
             }
             double red[NR];
+            float tf[NR];
 #pragma unroll
-            for (int j = 0; j < NR; j++) red[j] = 0.0;
+            for (int j = 0; j < NR; j++) {
+                red[j] = 0.0;
+                tf[j] = 0.f;
+            }
 
             if (k < kend) {
                 vec3<R> acc[NR];
@@ -206,8 +232,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) dslash_kernel(DslashArgs<LF, NR, 
                                            dot2(a.beta, acc[r].c[c].im, al, yv.c[c].im));
                         if (RED) {
 #pragma unroll
-                            for (int c = 0; c < 3; c++)
-                                red[r] += dot2((double)yv.c[c].re, (double)o.c[c].re, (double)yv.c[c].im, (double)o.c[c].im);
+                            for (int c = 0; c < 3; c++) site_dot(red[r], tf[r], yv.c[c], o.c[c]);
+                            if (sizeof(R) == 4) red[r] = (double)tf[r];
                         }
                     } else {
 #pragma unroll
@@ -232,9 +258,9 @@ template <class LF, int NR, bool RED>
 struct DsCand {
     typedef DslashCfg<LF, NR, RED> C;
     static constexpr int b0 = C::block, m0 = C::minb;
-    static constexpr bool def256 = b0 == 256, def1283 = b0 == 128 && m0 == 3;
-    static constexpr int b1 = def256 ? 128 : 256, m1 = def256 ? 4 : (def1283 ? 2 : 1);
-    static constexpr int b2 = 128, m2 = def256 ? 3 : (def1283 ? 4 : 3);
+    static constexpr bool def256 = b0 == 256, def1283 = b0 == 128 && m0 == 3, def1286 = b0 == 128 && m0 == 6;
+    static constexpr int b1 = def256 ? 128 : 256, m1 = def256 ? 4 : ((def1283 || def1286) ? 2 : 1);
+    static constexpr int b2 = 128, m2 = def256 ? 3 : ((def1283 || def1286) ? 4 : 3);
 };
 
 // Grid of a launch over nsites output sites: one block per tile of B sites, except for the
