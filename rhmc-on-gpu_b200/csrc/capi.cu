@@ -62,6 +62,7 @@ int rhmc_create(const rhmc_params *p, rhmc_ctx **out)
     c->g.nx = p->nx; c->g.ny = p->ny; c->g.nz = p->nz; c->g.nt = p->nt;
     c->g.Vh = (int)(V / 2);
     c->g.antiperiodic_t = p->ferm_temp_bc == 0;
+    geom_divisors(c->g);
     c->V = V; c->Vh = V / 2;
     c->device = p->device;
     c->mass = p->mass;

@@ -42,25 +42,63 @@ template <typename R> struct su3m { cpx<R> e[3][3]; };
 template <typename R> struct vec3 { cpx<R> c[3]; };
 
 // ------------------------------------------------------------------ lattice geometry
+// n / d for 0 <= n < 2^31 and d >= 2 as a multiply-high and a shift: with l = ceil(log2 d) and
+// m = ceil(2^(31+l) / d) (< 2^32), m d - 2^(31+l) < d <= 2^l, which keeps n m / 2^(31+l) within
+// the same integer as n / d for every n < 2^31 (the round-up method of Granlund and Montgomery,
+// "Division by invariant integers using multiplication", 1994).  A runtime integer division
+// compiles to some twenty instructions; site_of needs three per site.
+struct FastDiv {
+    unsigned m;
+    int s;  // l - 1
+};
+inline FastDiv make_fastdiv(unsigned d)
+{
+    int l = 0;
+    while ((1u << l) < d) l++;
+    FastDiv f;
+    f.m = (unsigned)((((unsigned long long)1 << (31 + l)) + d - 1) / d);
+    f.s = l - 1;
+    return f;
+}
+__host__ __device__ __forceinline__ unsigned fdiv(unsigned n, FastDiv f)
+{
+#ifdef __CUDA_ARCH__
+    return __umulhi(n, f.m) >> f.s;
+#else
+    return (unsigned)(((unsigned long long)n * f.m) >> 32) >> f.s;
+#endif
+}
+
 struct Geom {
     int nx, ny, nz, nt;
     int Vh;          // sites per parity
     int antiperiodic_t;  // 1: fermion phases flip on t = nt-1 (ferm_temp_bc == 0)
+    FastDiv dx, dy, dz;  // divisions by nx, ny, nz (set by geom_divisors)
 };
+
+// fills the divisors of g from its extents (every extent is even, hence >= 2)
+inline void geom_divisors(Geom &g)
+{
+    g.dx = make_fastdiv((unsigned)g.nx);
+    g.dy = make_fastdiv((unsigned)g.ny);
+    g.dz = make_fastdiv((unsigned)g.nz);
+}
 
 struct Site { int x, y, z, t; };
 
 // coordinates of (parity p, half index k)
 __host__ __device__ __forceinline__ Site site_of(const Geom &g, int p, int k)
 {
-    int lex2 = 2 * k;
-    int x0 = lex2 % g.nx;
-    int r = lex2 / g.nx;
+    const unsigned lex2 = 2u * (unsigned)k;
+    unsigned r = fdiv(lex2, g.dx);
+    const int x0 = (int)(lex2 - r * (unsigned)g.nx);
     Site s;
-    s.y = r % g.ny;
-    r /= g.ny;
-    s.z = r % g.nz;
-    s.t = r / g.nz;
+    unsigned q = fdiv(r, g.dy);
+    s.y = (int)(r - q * (unsigned)g.ny);
+    r = q;
+    q = fdiv(r, g.dz);
+    s.z = (int)(r - q * (unsigned)g.nz);
+    s.t = (int)q;
     s.x = x0 + ((p + x0 + s.y + s.z + s.t) & 1);
     return s;
 }

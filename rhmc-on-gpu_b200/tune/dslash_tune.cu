@@ -103,7 +103,8 @@ int main(int argc, char **argv)
     Only = argc > 4 && strcmp(argv[4], "all") ? argv[4] : nullptr;
     Persist = argc > 5 ? atoi(argv[5]) : 0;
     cudaDeviceGetAttribute(&NSM, cudaDevAttrMultiProcessorCount, 0);
-    G = Geom{nx, nx, nx, nt, nx * nx * nx * nt / 2, 1};
+    G = Geom{nx, nx, nx, nt, nx * nx * nx * nt / 2, 1, {}, {}, {}};
+    geom_divisors(G);
     const long Vh = G.Vh;
     printf("lattice %d^3x%d Vh=%ld\n", nx, nt, Vh);
     const size_t ub = (size_t)72 * Vh * 16, vb = (size_t)8 * 3 * Vh * 16;  // links FP64-18; 8 RHS FP64
